@@ -1,0 +1,858 @@
+/*
+ * oracle.c - CPU restatement of Pencil's per-pixel path-tracing loop.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker, never the product): see oracle.h
+ * for the list of reference functions restated here and their file:line.
+ * Every expression keeps the reference's float32 operation order so that,
+ * built with -ffp-contract=off, results match the reference bit for bit.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ---- Vec3 (src/vec3.hpp:24-92) ------------------------------------------ */
+typedef struct { float x, y, z; } v3;
+
+static inline v3 mk(float x, float y, float z) { v3 r = {x, y, z}; return r; }
+static inline v3 add(v3 a, v3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub(v3 a, v3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 neg(v3 a) { return mk(-a.x, -a.y, -a.z); }
+static inline v3 mulf(v3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+static inline v3 divf(v3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
+static inline v3 mulv(v3 a, v3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline v3 cross(v3 a, v3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline float len(v3 a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+static inline v3 nrm(v3 a) {
+    float l = len(a);
+    return (l > 1e-12f) ? divf(a, l) : mk(0.0f, 0.0f, 0.0f);
+}
+static inline v3 reflect(v3 v, v3 n) { return sub(v, mulf(n, 2.0f * dot(v, n))); }
+static inline float comp(v3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+static inline v3 ld3(const float* p) { return mk(p[0], p[1], p[2]); }
+static inline float clampf(float v, float lo, float hi) {
+    return (v < lo) ? lo : (v > hi) ? hi : v;
+}
+static inline float schlick(float c, float ratio) {
+    float r0 = (1.0f - ratio) / (1.0f + ratio);
+    r0 = r0 * r0;
+    return r0 + (1.0f - r0) * powf(1.0f - c, 5.0f);
+}
+
+/* ---- Rng (src/rng.hpp:13-45) --------------------------------------------- */
+typedef struct { uint32_t s; } rng_t;
+static inline uint32_t rng_u32(rng_t* r) {
+    r->s ^= r->s << 13u;
+    r->s ^= r->s >> 17u;
+    r->s ^= r->s << 5u;
+    return r->s;
+}
+static inline float rng_unit(rng_t* r) { return (float)rng_u32(r) / 4294967296.0f; }
+static inline float rng_sym(rng_t* r) { return rng_unit(r) * 2.0f - 1.0f; }
+static inline void rng_disc(rng_t* r, float* dx, float* dy) {
+    float r1 = rng_unit(r);
+    float r2 = rng_unit(r);
+    float sx = 2.0f * r1 - 1.0f;
+    float sy = 2.0f * r2 - 1.0f;
+    if (sx == 0.0f && sy == 0.0f) { *dx = 0; *dy = 0; return; }
+    float theta, rad;
+    if (fabsf(sx) > fabsf(sy)) {
+        rad = sx;
+        theta = (3.14159265f / 4.0f) * (sy / sx);
+    } else {
+        rad = sy;
+        theta = (3.14159265f / 2.0f) - (3.14159265f / 4.0f) * (sx / sy);
+    }
+    *dx = rad * cosf(theta);
+    *dy = rad * sinf(theta);
+}
+
+static uint32_t mix32(uint32_t x) {
+    x ^= x >> 16; x *= 0x7feb352dU;
+    x ^= x >> 15; x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
+uint32_t orc_path_seed(int32_t i, int32_t j, int32_t sample, uint32_t salt) {
+    uint32_t pix = (uint32_t)i * 97861u + (uint32_t)j * 1973u + 1u;
+    uint32_t s = mix32(pix ^ mix32((uint32_t)sample * 0x9E3779B9u + salt + 0x632BE5ABu));
+    return s ? s : 0x6D2B79F5u;
+}
+
+/* ---- hit record (src/primitives.hpp:70-81) ------------------------------- */
+typedef struct {
+    v3 p, n;
+    float t;
+    int mat;
+    int front;
+    int prim;
+} hitrec;
+
+typedef struct { v3 o, d; } ray_t;
+static inline v3 ray_at(ray_t r, float t) { return add(r.o, mulf(r.d, t)); }
+static inline void set_face(hitrec* h, ray_t r, v3 outward) {
+    h->front = dot(r.d, outward) < 0.0f;
+    h->n = h->front ? outward : neg(outward);
+}
+
+/* ---- primitives ---------------------------------------------------------- */
+static int hit_sphere(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec* h) {
+    v3 c = ld3(pr->p);
+    float rad = pr->p[3];
+    v3 oc = sub(r.o, c);
+    float a = dot(r.d, r.d);
+    float hb = dot(oc, r.d);
+    float cc = dot(oc, oc) - rad * rad;
+    float disc = hb * hb - a * cc;
+    if (disc < 0.0f) return 0;
+    float sq = sqrtf(disc);
+    float t = (-hb - sq) / a;
+    if (t < tmin || t > tmax) {
+        t = (-hb + sq) / a;
+        if (t < tmin || t > tmax) return 0;
+    }
+    h->t = t;
+    h->p = ray_at(r, t);
+    set_face(h, r, divf(sub(h->p, c), rad));
+    h->mat = pr->material;
+    return 1;
+}
+
+static int hit_triangle(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec* h) {
+    v3 v0 = ld3(pr->p), v1 = ld3(pr->p + 3), v2 = ld3(pr->p + 6);
+    v3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+    v3 hh = cross(r.d, e2);
+    float a = dot(e1, hh);
+    if (fabsf(a) < 1e-8f) return 0;
+    float f = 1.0f / a;
+    v3 s = sub(r.o, v0);
+    float u = f * dot(s, hh);
+    if (u < 0.0f || u > 1.0f) return 0;
+    v3 q = cross(s, e1);
+    float v = f * dot(r.d, q);
+    if (v < 0.0f || u + v > 1.0f) return 0;
+    float t = f * dot(e2, q);
+    if (t < tmin || t > tmax) return 0;
+    h->t = t;
+    h->p = ray_at(r, t);
+    set_face(h, r, nrm(cross(e1, e2)));
+    h->mat = pr->material;
+    return 1;
+}
+
+static int hit_cube(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec* h) {
+    v3 c = ld3(pr->p);
+    float hf = pr->p[3];
+    v3 lo = sub(c, mk(hf, hf, hf));
+    v3 hi = add(c, mk(hf, hf, hf));
+    float t_near = -INFINITY, t_far = INFINITY;
+    int near_axis = -1, far_axis = -1;
+    float near_sign = 1.0f, far_sign = -1.0f;
+    for (int a = 0; a < 3; ++a) {
+        const float d = comp(r.d, a);
+        const float o = comp(r.o, a);
+        if (fabsf(d) < 1e-12f) {
+            if (o < comp(lo, a) || o > comp(hi, a)) return 0;
+            continue;
+        }
+        float tn = (comp(lo, a) - o) / d;
+        float tf = (comp(hi, a) - o) / d;
+        float ns = -1.0f, fs = 1.0f;
+        if (tn > tf) { float x = tn; tn = tf; tf = x; x = ns; ns = fs; fs = x; }
+        if (tn > t_near) { t_near = tn; near_axis = a; near_sign = ns; }
+        if (tf < t_far) { t_far = tf; far_axis = a; far_sign = fs; }
+        if (t_far < t_near) return 0;
+    }
+    const int use_near = t_near >= tmin;
+    const float th = use_near ? t_near : t_far;
+    const int ax = use_near ? near_axis : far_axis;
+    const float sg = use_near ? near_sign : far_sign;
+    if (ax < 0 || th < tmin || th > tmax) return 0;
+    h->t = th;
+    h->p = ray_at(r, th);
+    v3 n = mk(0.0f, 0.0f, 0.0f);
+    if (ax == 0) n.x = sg; else if (ax == 1) n.y = sg; else n.z = sg;
+    set_face(h, r, n);
+    h->mat = pr->material;
+    return 1;
+}
+
+static int hit_plane(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec* h) {
+    v3 pt = ld3(pr->p), n = ld3(pr->p + 3);
+    float denom = dot(n, r.d);
+    if (fabsf(denom) < 1e-6f) return 0;
+    float t = dot(sub(pt, r.o), n) / denom;
+    if (t < tmin || t > tmax) return 0;
+    h->t = t;
+    h->p = ray_at(r, t);
+    set_face(h, r, n);
+    h->mat = pr->material;
+    return 1;
+}
+
+static int cyl_side(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec* h) {
+    v3 c = ld3(pr->p), ax = ld3(pr->p + 3);
+    float rad = pr->p[6], hh = pr->p[7];
+    v3 oc = sub(r.o, c);
+    float dda = dot(r.d, ax);
+    float oca = dot(oc, ax);
+    v3 dp = sub(r.d, mulf(ax, dda));
+    v3 op = sub(oc, mulf(ax, oca));
+    float a = dot(dp, dp);
+    float b = 2.0f * dot(op, dp);
+    float cc = dot(op, op) - rad * rad;
+    if (a < 1e-9f) {
+        if (fabsf(b) < 1e-9f) return 0;
+        const float t = -cc / b;
+        if (t < tmin || t > tmax) return 0;
+        const float hgt = oca + t * dda;
+        if (fabsf(hgt) > hh) return 0;
+        h->t = t;
+        h->p = ray_at(r, t);
+        v3 apt = add(c, mulf(ax, hgt));
+        set_face(h, r, divf(sub(h->p, apt), rad));
+        h->mat = pr->material;
+        return 1;
+    }
+    float disc = b * b - 4.0f * a * cc;
+    if (disc < 0.0f) return 0;
+    float sq = sqrtf(disc);
+    float ts[2];
+    ts[0] = (-b - sq) / (2.0f * a);
+    ts[1] = (-b + sq) / (2.0f * a);
+    for (int k = 0; k < 2; ++k) {
+        float t = ts[k];
+        if (t < tmin || t > tmax) continue;
+        float hgt = (oca + t * dda);
+        if (fabsf(hgt) > hh) continue;
+        h->t = t;
+        h->p = ray_at(r, t);
+        v3 apt = add(c, mulf(ax, hgt));
+        set_face(h, r, divf(sub(h->p, apt), rad));
+        h->mat = pr->material;
+        return 1;
+    }
+    return 0;
+}
+
+static int disc_cap(v3 center, v3 n, float rad, int mat, ray_t r, float tmin, float tmax, hitrec* h) {
+    float denom = dot(n, r.d);
+    if (fabsf(denom) < 1e-6f) return 0;
+    float t = dot(sub(center, r.o), n) / denom;
+    if (t < tmin || t > tmax) return 0;
+    v3 p = ray_at(r, t);
+    v3 d = sub(p, center);
+    if (dot(d, d) > rad * rad) return 0;
+    h->t = t;
+    h->p = p;
+    set_face(h, r, n);
+    h->mat = mat;
+    return 1;
+}
+
+static int hit_cylinder(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec* h) {
+    v3 c = ld3(pr->p), ax = ld3(pr->p + 3);
+    float rad = pr->p[6], hh = pr->p[7];
+    int found = 0;
+    float closest = tmax;
+    hitrec best;
+    if (cyl_side(pr, r, tmin, closest, &best)) { closest = best.t; *h = best; found = 1; }
+    if (disc_cap(add(c, mulf(ax, 1.0f * hh)), mulf(ax, 1.0f), rad, pr->material, r, tmin, closest, &best)) {
+        closest = best.t; *h = best; found = 1;
+    }
+    if (disc_cap(add(c, mulf(ax, -1.0f * hh)), mulf(ax, -1.0f), rad, pr->material, r, tmin, closest, &best)) {
+        closest = best.t; *h = best; found = 1;
+    }
+    return found;
+}
+
+static int cone_side(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec* h) {
+    v3 apex = ld3(pr->p), ax = ld3(pr->p + 3);
+    float rad = pr->p[6], hgt = pr->p[7];
+    v3 oc = sub(r.o, apex);
+    float dda = dot(r.d, ax);
+    float oca = dot(oc, ax);
+    float k = rad / hgt;
+    float k2 = k * k;
+    v3 dp = sub(r.d, mulf(ax, dda));
+    v3 op = sub(oc, mulf(ax, oca));
+    float a = dot(dp, dp) - k2 * dda * dda;
+    float b = 2.0f * (dot(dp, op) - k2 * dda * oca);
+    float cc = dot(op, op) - k2 * oca * oca;
+    float disc = b * b - 4.0f * a * cc;
+    if (disc < 0.0f || fabsf(a) < 1e-12f) return 0;
+    float sq = sqrtf(disc);
+    float ts[2];
+    ts[0] = (-b - sq) / (2.0f * a);
+    ts[1] = (-b + sq) / (2.0f * a);
+    for (int q = 0; q < 2; ++q) {
+        float t = ts[q];
+        if (t < tmin || t > tmax) continue;
+        float hh = oca + t * dda;
+        if (hh < 0.0f || hh > hgt) continue;
+        h->t = t;
+        h->p = ray_at(r, t);
+        v3 apt = add(apex, mulf(ax, hh));
+        v3 radial = sub(h->p, apt);
+        set_face(h, r, nrm(sub(nrm(radial), mulf(ax, k))));
+        h->mat = pr->material;
+        return 1;
+    }
+    return 0;
+}
+
+static int hit_cone(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec* h) {
+    v3 apex = ld3(pr->p), ax = ld3(pr->p + 3);
+    float rad = pr->p[6], hgt = pr->p[7];
+    v3 base = sub(apex, mulf(ax, hgt));
+    int found = 0;
+    float closest = tmax;
+    hitrec best;
+    if (cone_side(pr, r, tmin, closest, &best)) { closest = best.t; *h = best; found = 1; }
+    if (disc_cap(base, neg(ax), rad, pr->material, r, tmin, closest, &best)) {
+        closest = best.t; *h = best; found = 1;
+    }
+    return found;
+}
+
+static int hit_prim(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec* h) {
+    switch (pr->type) {
+        case PGPU_PRIM_SPHERE:   return hit_sphere(pr, r, tmin, tmax, h);
+        case PGPU_PRIM_TRIANGLE: return hit_triangle(pr, r, tmin, tmax, h);
+        case PGPU_PRIM_CUBE:     return hit_cube(pr, r, tmin, tmax, h);
+        case PGPU_PRIM_PLANE:    return hit_plane(pr, r, tmin, tmax, h);
+        case PGPU_PRIM_CYLINDER: return hit_cylinder(pr, r, tmin, tmax, h);
+        case PGPU_PRIM_CONE:     return hit_cone(pr, r, tmin, tmax, h);
+        default: return 0;
+    }
+}
+
+/* ---- BVH (src/bvh.hpp:31-48, AABB::hit src/primitives.hpp:38-49) -------- */
+static int box_hit(const pgpu_bvh_node* nd, ray_t r, float tmin, float tmax) {
+    for (int a = 0; a < 3; ++a) {
+        float inv = 1.0f / comp(r.d, a);
+        float t0 = (nd->bmin[a] - comp(r.o, a)) * inv;
+        float t1 = (nd->bmax[a] - comp(r.o, a)) * inv;
+        if (inv < 0.0f) { float x = t0; t0 = t1; t1 = x; }
+        tmin = (t0 > tmin) ? t0 : tmin;
+        tmax = (t1 < tmax) ? t1 : tmax;
+        if (tmax < tmin) return 0;
+    }
+    return 1;
+}
+
+typedef struct {
+    const orc_scene* s;
+    uint64_t* cnt;   /* may be NULL */
+} trav_t;
+
+static int node_hit(const trav_t* tv, int idx, ray_t r, float tmin, float tmax, hitrec* h) {
+    const pgpu_bvh_node* nd = &tv->s->nodes[idx];
+    if (tv->cnt) tv->cnt[ORC_CNT_NODE_VISITS]++;
+    if (!box_hit(nd, r, tmin, tmax)) return 0;
+    if (nd->left < 0) {
+        if (tv->cnt) tv->cnt[ORC_CNT_PRIM_TESTS]++;
+        int ok = hit_prim(&tv->s->prims[nd->right], r, tmin, tmax, h);
+        if (ok) h->prim = nd->right;
+        return ok;
+    }
+    int hl = node_hit(tv, nd->left, r, tmin, tmax, h);
+    int hr = node_hit(tv, nd->right, r, tmin, hl ? h->t : tmax, h);
+    return hl || hr;
+}
+
+static int node_occ(const trav_t* tv, int idx, ray_t r, float tmin, float tmax) {
+    const pgpu_bvh_node* nd = &tv->s->nodes[idx];
+    if (tv->cnt) tv->cnt[ORC_CNT_NODE_VISITS]++;
+    if (!box_hit(nd, r, tmin, tmax)) return 0;
+    if (nd->left < 0) {
+        hitrec tmp;
+        if (tv->cnt) tv->cnt[ORC_CNT_PRIM_TESTS]++;
+        return hit_prim(&tv->s->prims[nd->right], r, tmin, tmax, &tmp);
+    }
+    if (node_occ(tv, nd->left, r, tmin, tmax)) return 1;
+    if (node_occ(tv, nd->right, r, tmin, tmax)) return 1;
+    return 0;
+}
+
+/* Scene::hit / Scene::occluded (src/scene.hpp:55-81), BVH branch. */
+static int scene_hit(const trav_t* tv, ray_t r, float tmin, float tmax, hitrec* h) {
+    if (tv->cnt) tv->cnt[ORC_CNT_EXTENSION_RAYS]++;
+    if (tv->s->n_nodes <= 0) return 0;
+    return node_hit(tv, 0, r, tmin, tmax, h);
+}
+static int scene_occ(const trav_t* tv, ray_t r, float tmin, float tmax) {
+    if (tv->cnt) tv->cnt[ORC_CNT_SHADOW_RAYS]++;
+    if (tv->s->n_nodes <= 0) return 0;
+    return node_occ(tv, 0, r, tmin, tmax);
+}
+
+/* ---- camera (src/camera.hpp:67-86, src/camera.cpp:48-68) ---------------- */
+void orc_camera_basis(const pgpu_camera* c, float out[21]) {
+    v3 eye = ld3(c->eye), look = ld3(c->look), up = ld3(c->up);
+    v3 w = nrm(sub(eye, look));
+    v3 u = nrm(cross(up, w));
+    v3 v = cross(w, u);
+    float theta = c->vfov_deg * 3.14159265358979323846f / 180.0f;
+    float half_h = tanf(theta * 0.5f);
+    float half_w = c->aspect * half_h;
+    v3 hor = mulf(u, 2.0f * half_w * c->focus_dist);
+    v3 ver = mulf(v, 2.0f * half_h * c->focus_dist);
+    v3 ll = sub(sub(sub(eye, mulf(hor, 0.5f)), mulf(ver, 0.5f)), mulf(w, c->focus_dist));
+    v3 all[7] = {eye, ll, hor, ver, u, v, w};
+    for (int k = 0; k < 7; ++k) {
+        out[3 * k + 0] = all[k].x; out[3 * k + 1] = all[k].y; out[3 * k + 2] = all[k].z;
+    }
+}
+
+static ray_t camera_ray(const orc_scene* s, float u, float v) {
+    v3 org = ld3(s->cam), ll = ld3(s->cam + 3), hor = ld3(s->cam + 6), ver = ld3(s->cam + 9);
+    v3 dir = sub(add(add(ll, mulf(hor, u)), mulf(ver, v)), org);
+    ray_t r = {org, nrm(dir)};
+    return r;
+}
+
+/* ---- shading ------------------------------------------------------------- */
+typedef struct {
+    const orc_scene* s;
+    const pgpu_render_params* p;
+    trav_t tv;
+    uint64_t* cnt;
+} ctx_t;
+
+/* Light direction for one light at p (soft disc jitter included):
+ * src/renderer.hpp:512-545 and 887-906 share this computation. */
+static void light_dir(const pgpu_light* l, v3 p, rng_t* rng, v3* L, float* dist) {
+    v3 lpos = ld3(l->pos);
+    if (l->kind == PGPU_LIGHT_POINT && l->radius > 0.0f) {
+        v3 to = sub(ld3(l->pos), p);
+        v3 axis = nrm(to);
+        v3 upv = (fabsf(axis.y) < 0.9f) ? mk(0, 1, 0) : mk(1, 0, 0);
+        v3 t1 = nrm(cross(axis, upv));
+        v3 t2 = nrm(cross(axis, t1));
+        float dx, dy;
+        rng_disc(rng, &dx, &dy);
+        lpos = add(ld3(l->pos), mulf(add(mulf(t1, dx), mulf(t2, dy)), l->radius));
+    }
+    if (l->kind == PGPU_LIGHT_POINT) {
+        v3 d = sub(lpos, p);
+        *dist = len(d);
+        *L = divf(d, *dist);
+    } else {
+        *L = neg(ld3(l->pos));
+        *dist = 1e9f;
+    }
+}
+
+static v3 whitted(ctx_t* c, ray_t r, int depth, rng_t* rng);
+
+static v3 dielectric(ctx_t* c, ray_t r, const hitrec* rec, const pgpu_material* m,
+                     v3 albedo, int depth, rng_t* rng) {
+    float bias = c->p->shadow_bias;
+    float ior = m->ior;
+    int entering = rec->front;
+    float safe = fmaxf(ior, 0.01f);
+    float eta = entering ? (1.0f / safe) : safe;
+    v3 nf = rec->n;
+    float cos_i = fabsf(dot(nrm(r.d), rec->n));
+    float sin_t2 = eta * eta * (1.0f - cos_i * cos_i);
+    v3 rdir = nrm(reflect(nrm(r.d), rec->n));
+    ray_t rr = {add(rec->p, mulf(rec->n, bias)), rdir};
+    v3 rc = whitted(c, rr, depth - 1, rng);
+    if (sin_t2 > 1.0f) return mulv(rc, albedo);
+    float cos_t = sqrtf(1.0f - sin_t2);
+    v3 tdir = nrm(add(mulf(nrm(r.d), eta), mulf(nf, eta * cos_i - cos_t)));
+    ray_t tr = {sub(rec->p, mulf(nf, bias)), tdir};
+    v3 tc = whitted(c, tr, depth - 1, rng);
+    float cf = entering ? cos_i : cos_t;
+    float kr = schlick(cf, eta);
+    float kt = 1.0f - kr;
+    v3 g = add(mulf(rc, kr), mulf(tc, kt));
+    return mulv(g, albedo);
+}
+
+static v3 whitted(ctx_t* c, ray_t r, int depth, rng_t* rng) {
+    const orc_scene* s = c->s;
+    float bias = c->p->shadow_bias;
+    if (c->cnt) c->cnt[ORC_CNT_REFERENCE_RAYS]++;
+    if (depth <= 0) return mk(0, 0, 0);
+    hitrec rec;
+    if (!scene_hit(&c->tv, r, 1e-4f, 1e9f, &rec)) return ld3(s->background);
+    const pgpu_material* m = &s->materials[rec.mat];
+    v3 albedo = ld3(m->albedo);
+    v3 sn = rec.n;
+    v3 local = ld3(m->emission);
+    for (int li = 0; li < s->n_lights; ++li) {
+        const pgpu_light* l = &s->lights[li];
+        if (l->kind == PGPU_LIGHT_QUAD) continue;
+        v3 contrib = mk(0, 0, 0);
+        int ns = (l->radius > 0.0f) ? c->p->soft_shadow_samples : 1;
+        for (int k = 0; k < ns; ++k) {
+            v3 L; float dist;
+            light_dir(l, rec.p, rng, &L, &dist);
+            ray_t sr = {add(rec.p, mulf(rec.n, bias)), L};
+            if (!l->is_emissive && scene_occ(&c->tv, sr, bias, dist - bias)) continue;
+            float ndotl = clampf(dot(sn, L), 0.0f, 1.0f);
+            v3 col = mulf(mulv(albedo, ld3(l->intensity)), ndotl);
+            if (m->specular > 0.0f && ndotl > 0.0f) {
+                v3 V = neg(nrm(r.d));
+                v3 H = nrm(add(L, V));
+                float ndoth = clampf(dot(sn, H), 0.0f, 1.0f);
+                float spec = powf(ndoth, m->shininess);
+                col = add(col, mulf(mulv(ld3(m->specular_color), ld3(l->intensity)), spec * m->specular));
+            }
+            contrib = add(contrib, col);
+        }
+        local = add(local, divf(contrib, (float)ns));
+    }
+    local = add(local, mulv(albedo, ld3(s->ambient)));
+    if (m->kind == PGPU_MAT_METAL && m->reflectivity > 0.0f) {
+        v3 rd = nrm(reflect(nrm(r.d), rec.n));
+        ray_t rr = {add(rec.p, mulf(rec.n, bias)), rd};
+        v3 inc = whitted(c, rr, depth - 1, rng);
+        v3 refl = mulf(mulv(inc, albedo), m->reflectivity);
+        local = add(mulf(local, 1.0f - m->reflectivity), refl);
+    } else if (m->kind == PGPU_MAT_DIELECTRIC) {
+        local = dielectric(c, r, &rec, m, albedo, depth, rng);
+    }
+    return local;
+}
+
+static v3 trace_path(ctx_t* c, ray_t r, int bounces, rng_t* rng) {
+    const orc_scene* s = c->s;
+    float bias = c->p->shadow_bias;
+    if (c->cnt) c->cnt[ORC_CNT_REFERENCE_RAYS]++;
+    v3 T = mk(1, 1, 1);
+    v3 rad = mk(0, 0, 0);
+    ray_t cur = r;
+    int depth = bounces;
+    while (depth > 0) {
+        hitrec rec;
+        if (!scene_hit(&c->tv, cur, 1e-4f, 1e9f, &rec)) {
+            rad = add(rad, mulv(T, ld3(s->background)));
+            break;
+        }
+        const pgpu_material* m = &s->materials[rec.mat];
+        rad = add(rad, mulv(T, ld3(m->emission)));
+        v3 albedo = ld3(m->albedo);
+        v3 sn = rec.n;
+        for (int li = 0; li < s->n_lights; ++li) {
+            const pgpu_light* l = &s->lights[li];
+            if (l->kind == PGPU_LIGHT_QUAD) continue;
+            v3 L; float dist;
+            light_dir(l, rec.p, rng, &L, &dist);
+            ray_t sr = {add(rec.p, mulf(rec.n, bias)), L};
+            if (!l->is_emissive && scene_occ(&c->tv, sr, bias, dist - bias)) continue;
+            float ndotl = clampf(dot(sn, L), 0.0f, 1.0f);
+            rad = add(rad, mulf(mulv(mulv(T, albedo), ld3(l->intensity)), ndotl));
+        }
+        rad = add(rad, mulv(mulv(T, albedo), ld3(s->ambient)));
+        if (bounces - depth > 3) {
+            float p = fmaxf(T.x, fmaxf(T.y, T.z));
+            if (rng_unit(rng) > p) break;
+            T = divf(T, p);
+        }
+        v3 nd;
+        v3 nT = mulv(T, albedo);
+        if (m->kind == PGPU_MAT_METAL && m->reflectivity > 0.0f) {
+            v3 refl = nrm(reflect(nrm(cur.d), sn));
+            v3 upv = (fabsf(refl.y) < 0.9f) ? mk(0, 1, 0) : mk(1, 0, 0);
+            v3 t1 = nrm(cross(refl, upv));
+            v3 t2 = nrm(cross(refl, t1));
+            float r1 = rng_unit(rng) * 0.1f;
+            float r2 = rng_unit(rng) * 6.28f;
+            nd = nrm(add(add(refl, mulf(t1, r1 * cosf(r2))), mulf(t2, r1 * sinf(r2))));
+            nT = mulf(mulv(T, albedo), m->reflectivity);
+        } else if (m->kind == PGPU_MAT_DIELECTRIC) {
+            v3 g = dielectric(c, cur, &rec, m, albedo, depth, rng);
+            rad = add(rad, sub(mulv(T, g), mulv(T, ld3(m->emission))));
+            break;
+        } else {
+            float r1 = rng_unit(rng) * 6.2831853f;
+            float r2 = rng_unit(rng);
+            float r2s = sqrtf(r2);
+            v3 N = sn;
+            v3 upv = (fabsf(N.y) < 0.9f) ? mk(0, 1, 0) : mk(1, 0, 0);
+            v3 Tn = nrm(cross(upv, N));
+            v3 B = nrm(cross(N, Tn));
+            nd = nrm(add(add(mulf(mulf(Tn, cosf(r1)), r2s), mulf(mulf(B, sinf(r1)), r2s)),
+                         mulf(N, sqrtf(1.0f - r2))));
+        }
+        cur.o = add(rec.p, mulf(rec.n, bias));
+        cur.d = nd;
+        T = nT;
+        depth--;
+    }
+    return rad;
+}
+
+/* ---- render_tile_region (src/renderer.hpp:309-390) ----------------------- */
+typedef struct {
+    const orc_scene* s;
+    const pgpu_render_params* p;
+    float* out;
+    float* m2;
+    int row0, stride;    /* rows row0, row0 + stride, ... */
+    uint64_t cnt[ORC_CNT_N];
+} job_t;
+
+static void render_pixel(const job_t* jb, ctx_t* c, int i, int j) {
+    const pgpu_render_params* p = jb->p;
+    const int W = p->width, H = p->height, n = p->samples;
+    rng_t rng = {(uint32_t)(i * 97861u + j * 1973u + 1u)};
+    v3 acc = mk(0, 0, 0);
+    v3 sq = mk(0, 0, 0);
+    for (int sy = 0; sy < n; ++sy) {
+        for (int sx = 0; sx < n; ++sx) {
+            float u = (i + (sx + 0.5f) / n) / (float)W;
+            float v = 1.0f - (j + (sy + 0.5f) / n) / (float)H;
+            u += rng_sym(&rng) * (0.5f / (W * n));
+            v += rng_sym(&rng) * (0.5f / (H * n));
+            ray_t r = camera_ray(jb->s, u, v);
+            v3 col = (p->mode == PGPU_MODE_PATHTRACE) ? trace_path(c, r, p->depth, &rng)
+                                                      : whitted(c, r, p->depth, &rng);
+            acc = add(acc, col);
+            sq = add(sq, mulv(col, col));
+        }
+    }
+    acc = divf(acc, (float)(n * n));
+    size_t o = ((size_t)j * W + i) * 3;
+    jb->out[o + 0] = acc.x; jb->out[o + 1] = acc.y; jb->out[o + 2] = acc.z;
+    if (jb->m2) {
+        sq = divf(sq, (float)(n * n));
+        jb->m2[o + 0] = sq.x; jb->m2[o + 1] = sq.y; jb->m2[o + 2] = sq.z;
+    }
+}
+
+static void* render_thread(void* arg) {
+    job_t* jb = (job_t*)arg;
+    ctx_t c;
+    c.s = jb->s;
+    c.p = jb->p;
+    c.cnt = jb->cnt;
+    c.tv.s = jb->s;
+    c.tv.cnt = jb->cnt;
+    for (int j = jb->row0; j < jb->p->height; j += jb->stride)
+        for (int i = 0; i < jb->p->width; ++i) render_pixel(jb, &c, i, j);
+    return NULL;
+}
+
+int32_t orc_render(const orc_scene* s, const pgpu_render_params* p, float* out_rgb,
+                   float* out_m2, int32_t n_threads, uint64_t* counters) {
+    if (!s || !p || !out_rgb || p->width <= 0 || p->height <= 0 || p->samples <= 0) return -1;
+    if (p->mode != PGPU_MODE_PATHTRACE && p->mode != PGPU_MODE_WHITTED) return -1;
+    if (n_threads < 1) n_threads = 1;
+    if (n_threads > p->height) n_threads = p->height;
+    job_t* jobs = (job_t*)calloc((size_t)n_threads, sizeof(job_t));
+    pthread_t* th = (pthread_t*)calloc((size_t)n_threads, sizeof(pthread_t));
+    char* live = (char*)calloc((size_t)n_threads, 1);
+    for (int k = 0; k < n_threads; ++k) {
+        jobs[k].s = s; jobs[k].p = p; jobs[k].out = out_rgb; jobs[k].m2 = out_m2;
+        jobs[k].row0 = k; jobs[k].stride = n_threads;
+    }
+    for (int k = 1; k < n_threads; ++k)
+        live[k] = pthread_create(&th[k], NULL, render_thread, &jobs[k]) == 0;
+    render_thread(&jobs[0]);
+    for (int k = 1; k < n_threads; ++k) {
+        if (live[k]) pthread_join(th[k], NULL);
+        else render_thread(&jobs[k]);
+    }
+    if (counters) {
+        for (int q = 0; q < ORC_CNT_N; ++q) {
+            uint64_t acc = 0;
+            for (int k = 0; k < n_threads; ++k) acc += jobs[k].cnt[q];
+            counters[q] = acc;
+        }
+    }
+    free(live);
+    free(jobs);
+    free(th);
+    return 0;
+}
+
+/* ---- ray queries ---------------------------------------------------------- */
+void orc_trace_rays(const orc_scene* s, const float* rays, int32_t n, int32_t* prim_id,
+                    float* t, uint64_t* counters) {
+    trav_t tv = {s, counters};
+    for (int k = 0; k < n; ++k) {
+        ray_t r = {ld3(rays + 6 * k), ld3(rays + 6 * k + 3)};
+        hitrec h;
+        h.prim = -1;
+        if (scene_hit(&tv, r, 1e-4f, 1e9f, &h)) {
+            prim_id[k] = h.prim;
+            t[k] = h.t;
+        } else {
+            prim_id[k] = -1;
+            t[k] = -1.0f;
+        }
+    }
+}
+
+void orc_camera_rays(const orc_scene* s, const float* uv, int32_t n, float* rays) {
+    for (int k = 0; k < n; ++k) {
+        ray_t r = camera_ray(s, uv[2 * k], uv[2 * k + 1]);
+        rays[6 * k + 0] = r.o.x; rays[6 * k + 1] = r.o.y; rays[6 * k + 2] = r.o.z;
+        rays[6 * k + 3] = r.d.x; rays[6 * k + 4] = r.d.y; rays[6 * k + 5] = r.d.z;
+    }
+}
+
+void orc_primary_hits(const orc_scene* s, const float* uv, int32_t n, int32_t* prim_id, float* t) {
+    trav_t tv = {s, NULL};
+    for (int k = 0; k < n; ++k) {
+        ray_t r = camera_ray(s, uv[2 * k], uv[2 * k + 1]);
+        hitrec h;
+        if (scene_hit(&tv, r, 1e-4f, 1e9f, &h)) {
+            prim_id[k] = h.prim;
+            t[k] = h.t;
+        } else {
+            prim_id[k] = -1;
+            t[k] = -1.0f;
+        }
+    }
+}
+
+/* ---- FP64 hit distance recomputation -------------------------------------- */
+typedef struct { double x, y, z; } d3;
+static inline d3 dk(double x, double y, double z) { d3 r = {x, y, z}; return r; }
+static inline d3 dsub(d3 a, d3 b) { return dk(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline d3 dadd(d3 a, d3 b) { return dk(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline d3 dmul(d3 a, double s) { return dk(a.x * s, a.y * s, a.z * s); }
+static inline double ddot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline d3 dcross(d3 a, d3 b) {
+    return dk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline d3 dld(const float* p) { return dk(p[0], p[1], p[2]); }
+static inline double dcomp(d3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+
+static int quad_roots(double a, double b, double c, double* t0, double* t1) {
+    double disc = b * b - 4.0 * a * c;
+    if (disc < 0.0 || a == 0.0) return 0;
+    double sq = sqrt(disc);
+    *t0 = (-b - sq) / (2.0 * a);
+    *t1 = (-b + sq) / (2.0 * a);
+    return 1;
+}
+
+static double best_of(double cur, double t) {
+    if (t < 1e-4 || t > 1e9) return cur;
+    if (cur < 0.0 || t < cur) return t;
+    return cur;
+}
+
+double orc_hit_t_fp64(const pgpu_prim* pr, const float* rayf) {
+    d3 o = dld(rayf), d = dld(rayf + 3);
+    double best = -1.0;
+    switch (pr->type) {
+        case PGPU_PRIM_SPHERE: {
+            d3 c = dld(pr->p);
+            double r = pr->p[3];
+            d3 oc = dsub(o, c);
+            double t0, t1;
+            if (quad_roots(ddot(d, d), 2.0 * ddot(oc, d), ddot(oc, oc) - r * r, &t0, &t1)) {
+                best = best_of(best, t0);
+                if (best < 0.0) best = best_of(best, t1);
+            }
+            return best;
+        }
+        case PGPU_PRIM_TRIANGLE: {
+            d3 v0 = dld(pr->p), v1 = dld(pr->p + 3), v2 = dld(pr->p + 6);
+            d3 e1 = dsub(v1, v0), e2 = dsub(v2, v0);
+            d3 n = dcross(e1, e2);
+            double den = ddot(n, d);
+            if (den == 0.0) return -1.0;
+            double t = ddot(dsub(v0, o), n) / den;
+            return best_of(best, t);
+        }
+        case PGPU_PRIM_PLANE: {
+            d3 pt = dld(pr->p), n = dld(pr->p + 3);
+            double den = ddot(n, d);
+            if (den == 0.0) return -1.0;
+            return best_of(best, ddot(dsub(pt, o), n) / den);
+        }
+        case PGPU_PRIM_CUBE: {
+            d3 c = dld(pr->p);
+            double h = pr->p[3];
+            double tn = -INFINITY, tf = INFINITY;
+            for (int a = 0; a < 3; ++a) {
+                double da = dcomp(d, a), oa = dcomp(o, a), ca = dcomp(c, a);
+                if (da == 0.0) {
+                    if (oa < ca - h || oa > ca + h) return -1.0;
+                    continue;
+                }
+                double t0 = (ca - h - oa) / da, t1 = (ca + h - oa) / da;
+                if (t0 > t1) { double x = t0; t0 = t1; t1 = x; }
+                if (t0 > tn) tn = t0;
+                if (t1 < tf) tf = t1;
+            }
+            if (tf < tn) return -1.0;
+            best = best_of(best, tn);
+            if (best < 0.0) best = best_of(best, tf);
+            return best;
+        }
+        case PGPU_PRIM_CYLINDER:
+        case PGPU_PRIM_CONE: {
+            d3 c = dld(pr->p), ax = dld(pr->p + 3);
+            double rad = pr->p[6], hp = pr->p[7];
+            d3 oc = dsub(o, c);
+            double dda = ddot(d, ax), oca = ddot(oc, ax);
+            d3 dp = dsub(d, dmul(ax, dda)), op = dsub(oc, dmul(ax, oca));
+            double t0, t1, a, b, cc;
+            int cyl = pr->type == PGPU_PRIM_CYLINDER;
+            double k2 = cyl ? 0.0 : (rad / hp) * (rad / hp);
+            a = ddot(dp, dp) - k2 * dda * dda;
+            b = 2.0 * (ddot(op, dp) - k2 * dda * oca);
+            cc = ddot(op, op) - (cyl ? rad * rad : k2 * oca * oca);
+            if (quad_roots(a, b, cc, &t0, &t1)) {
+                double ts[2] = {t0, t1};
+                for (int q = 0; q < 2; ++q) {
+                    double hh = oca + ts[q] * dda;
+                    int ok = cyl ? fabs(hh) <= hp : (hh >= 0.0 && hh <= hp);
+                    if (ok && ts[q] >= 1e-4 && ts[q] <= 1e9) { best = best_of(best, ts[q]); break; }
+                }
+            }
+            /* caps */
+            int ncap = cyl ? 2 : 1;
+            for (int q = 0; q < ncap; ++q) {
+                double sg = cyl ? (q == 0 ? 1.0 : -1.0) : -1.0;
+                d3 cc3 = cyl ? dadd(c, dmul(ax, sg * hp)) : dsub(c, dmul(ax, hp));
+                d3 n = dmul(ax, sg);
+                double den = ddot(n, d);
+                if (den == 0.0) continue;
+                double t = ddot(dsub(cc3, o), n) / den;
+                d3 pp = dadd(o, dmul(d, t));
+                d3 dd = dsub(pp, cc3);
+                if (ddot(dd, dd) <= rad * rad) best = best_of(best, t);
+            }
+            return best;
+        }
+        default:
+            return -1.0;
+    }
+}
+
+/* ---- write_image's HDR -> 8-bit path (src/image_io.hpp:63-113) ----------- */
+static float aces(float x) {
+    float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+    float y = (x * (a * x + b)) / (x * (c * x + d) + e);
+    return y > 0.0f ? y : 0.0f;
+}
+
+void orc_rgb8(const float* hdr, int32_t n_pixels, uint8_t* out, int32_t tonemap, float exposure) {
+    float e = powf(2.0f, exposure);
+    for (int k = 0; k < n_pixels; ++k) {
+        for (int ch = 0; ch < 3; ++ch) {
+            float x = hdr[3 * k + ch] * e;
+            if (tonemap == 1) x = aces(x);
+            else if (tonemap == 2) x = x / (1.0f + x);
+            x = clampf(x, 0.0f, 1.0f);
+            x = powf(x, 1.0f / 2.2f);
+            out[3 * k + ch] = (uint8_t)(x * 255.0f + 0.5f);
+        }
+    }
+}

@@ -1,0 +1,833 @@
+// api.cu - the C-ABI of libpencil_gpu.so (include/pencil_gpu.h): contexts,
+// scene upload (validation and conversion of Pencil's DFS BVH into the
+// device layout of scene_layout.h), render dispatch and ray queries.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "host_internal.h"
+
+namespace pgpu {
+
+cudaError_t launch_megakernel(const SceneView& S, const RenderCfg& c, float* out, float* m2,
+                              unsigned long long* counters, cudaStream_t st);
+cudaError_t launch_query(const SceneView& S, bool camera, const float* in, int n, int* prim,
+                         float* t, cudaStream_t st);
+
+struct WfScratch;
+WfScratch* wavefront_new();
+void wavefront_delete(WfScratch* W);
+cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
+                             const std::vector<std::vector<DevLight>>& lights,
+                             const std::vector<int>& job_view, const std::vector<RenderCfg>& cfgs,
+                             const std::vector<float*>& outs, const std::vector<float*>& m2s,
+                             unsigned long long* counters, cudaStream_t st, bool use_graph,
+                             int* launches, int* status_out);
+
+constexpr int kMaxDepth = 64;          // traversal stack bound (kMaxStack)
+constexpr int kMaxTreeFrames = 32;     // Whitted recursion bound of the two-branch mode
+
+struct DeviceScene {
+    void* arena = nullptr;
+    size_t bytes = 0;
+    SceneView view{};
+    int n_unified = 0;
+    int n_leaves = 0;
+    int depth = 0;
+    std::vector<DevMaterial> mats;
+    std::vector<DevLight> lights;
+    std::vector<int> quad_mats;        // material ids of quad-light emitters
+    DevMaterial* d_mats = nullptr;
+};
+
+// Host mirror of Pencil's Vec3 arithmetic (src/vec3.hpp), for the camera
+// basis: compiled with -ffp-contract=off, it rounds as the reference does.
+struct HV {
+    float x, y, z;
+};
+static inline HV hv(const float* p) { return HV{p[0], p[1], p[2]}; }
+static inline HV operator+(HV a, HV b) { return HV{a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline HV operator-(HV a, HV b) { return HV{a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline HV operator*(HV a, float s) { return HV{a.x * s, a.y * s, a.z * s}; }
+static inline HV hcross(HV a, HV b) {
+    return HV{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+static inline HV hnorm(HV a) {
+    float l = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+    return (l > 1e-12f) ? HV{a.x / l, a.y / l, a.z / l} : HV{0.0f, 0.0f, 0.0f};
+}
+
+// Camera constructor: recompute_basis + recompute_frustum (src/camera.hpp:67-86).
+static void camera_basis(const pgpu_camera& c, float out[21]) {
+    HV eye = hv(c.eye), look = hv(c.look), up = hv(c.up);
+    HV w = hnorm(eye - look);
+    HV u = hnorm(hcross(up, w));
+    HV v = hcross(w, u);
+    float theta = c.vfov_deg * 3.14159265358979323846f / 180.0f;
+    float half_h = std::tan(theta * 0.5f);
+    float half_w = c.aspect * half_h;
+    HV hor = u * (2.0f * half_w * c.focus_dist);
+    HV ver = v * (2.0f * half_h * c.focus_dist);
+    HV ll = eye - hor * 0.5f - ver * 0.5f - w * c.focus_dist;
+    HV all[7] = {eye, ll, hor, ver, u, v, w};
+    for (int k = 0; k < 7; ++k) {
+        out[3 * k] = all[k].x;
+        out[3 * k + 1] = all[k].y;
+        out[3 * k + 2] = all[k].z;
+    }
+}
+
+static inline bool finite3(const float* p) {
+    return std::isfinite(p[0]) && std::isfinite(p[1]) && std::isfinite(p[2]);
+}
+
+}  // namespace pgpu
+
+using namespace pgpu;
+
+struct pgpu_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::map<int, std::unique_ptr<DeviceScene>> scenes;
+    int next_id = 1;
+    float* d_out = nullptr;
+    size_t out_cap = 0;
+    float* d_m2 = nullptr;
+    size_t m2_cap = 0;
+    unsigned long long* d_cnt = nullptr;
+    void* d_query = nullptr;
+    size_t query_cap = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    WfScratch* wf = nullptr;
+    int* h_status = nullptr;          // pinned
+};
+
+namespace {
+
+int fail(pgpu_ctx* c, int code, const char* fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        std::vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+
+int cuda_fail(pgpu_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, PGPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define PGPU_CUDA(ctx, call)                                          \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);    \
+    } while (0)
+
+template <typename T>
+int ensure(pgpu_ctx* c, T*& ptr, size_t& cap, size_t need) {
+    if (cap >= need && ptr) return PGPU_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr), std::max<size_t>(need, 256));
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return fail(c, PGPU_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu): %s", need, cudaGetErrorString(e));
+    }
+    cap = std::max<size_t>(need, 256);
+    return PGPU_OK;
+}
+
+DeviceScene* find_scene(pgpu_ctx* c, int id) {
+    auto it = c->scenes.find(id);
+    return it == c->scenes.end() ? nullptr : it->second.get();
+}
+
+// Validate Pencil's DFS node table against the unified primitive count:
+// node 0 is the root, an interior node's left child is the next node and its
+// right child comes later, every primitive is the leaf of exactly one node.
+int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims, int& depth) {
+    depth = 0;
+    if (n_prims == 0) {
+        if (n_nodes != 0) return fail(c, PGPU_ERR_BVH_INVALID, "nodes given for an empty scene");
+        return PGPU_OK;
+    }
+    if (n_nodes != 2 * n_prims - 1)
+        return fail(c, PGPU_ERR_BVH_INVALID, "%d nodes for %d primitives (need 2n-1)", n_nodes,
+                    n_prims);
+    std::vector<char> seen_prim(n_prims, 0);
+    std::vector<std::pair<int, int>> st;   // node, level
+    st.push_back({0, 1});
+    int visited = 0;
+    while (!st.empty()) {
+        auto [k, lvl] = st.back();
+        st.pop_back();
+        if (k < 0 || k >= n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "node index %d out of range", k);
+        // popping left before right visits nodes in pre-order: the table must
+        // list them in exactly that order
+        if (k != visited)
+            return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
+        ++visited;
+        depth = std::max(depth, lvl);
+        const pgpu_bvh_node& nd = nodes[k];
+        if (!finite3(nd.bmin) || !finite3(nd.bmax))
+            return fail(c, PGPU_ERR_BVH_INVALID, "node %d has a non-finite box", k);
+        if (nd.left < 0) {
+            if (nd.right < 0 || nd.right >= n_prims)
+                return fail(c, PGPU_ERR_BVH_INVALID, "leaf %d references primitive %d", k, nd.right);
+            if (seen_prim[nd.right]++)
+                return fail(c, PGPU_ERR_BVH_INVALID, "primitive %d is in two leaves", nd.right);
+        } else {
+            if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes)
+                return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
+            st.push_back({nd.right, lvl + 1});
+            st.push_back({nd.left, lvl + 1});
+        }
+        if (visited > n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "node table has a cycle");
+    }
+    if (visited != n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "unreachable nodes in table");
+    if (depth > kMaxDepth)
+        return fail(c, PGPU_ERR_UNSUPPORTED, "BVH depth %d exceeds %d", depth, kMaxDepth);
+    return PGPU_OK;
+}
+
+int check_prim(pgpu_ctx* c, const pgpu_prim& p, int k, int n_mat) {
+    if (p.type < PGPU_PRIM_SPHERE || p.type > PGPU_PRIM_CONE)
+        return fail(c, PGPU_ERR_UNSUPPORTED, "primitive %d has unsupported type %d", k, p.type);
+    if (p.material < 0 || p.material >= n_mat)
+        return fail(c, PGPU_ERR_INVALID_ARG, "primitive %d uses material %d of %d", k, p.material, n_mat);
+    for (int q = 0; q < 14; ++q)
+        if (!std::isfinite(p.p[q]))
+            return fail(c, PGPU_ERR_INVALID_ARG, "primitive %d has a non-finite parameter", k);
+    return PGPU_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" {
+
+int32_t pgpu_abi_version(void) { return PGPU_ABI_VERSION; }
+
+int32_t pgpu_create(int32_t device, pgpu_ctx** out) {
+    if (!out) return PGPU_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return PGPU_ERR_CUDA;
+    if (device < 0 || device >= n) return PGPU_ERR_INVALID_ARG;
+    auto* c = new pgpu_ctx();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void**>(&c->d_cnt), CNT_N * sizeof(unsigned long long)) !=
+            cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&c->h_status), 16) != cudaSuccess) {
+        pgpu_destroy(c);
+        return PGPU_ERR_CUDA;
+    }
+    c->stream = c->own;
+    c->wf = wavefront_new();
+    *out = c;
+    return PGPU_OK;
+}
+
+void pgpu_destroy(pgpu_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& kv : c->scenes) cudaFree(kv.second->arena);
+    c->scenes.clear();
+    cudaFree(c->d_out);
+    cudaFree(c->d_m2);
+    cudaFree(c->d_cnt);
+    cudaFree(c->d_query);
+    wavefront_delete(c->wf);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+}
+
+const char* pgpu_last_error(const pgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int32_t pgpu_set_stream(pgpu_ctx* c, void* stream) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own;
+    return PGPU_OK;
+}
+
+void* pgpu_get_stream(pgpu_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int32_t pgpu_make_prim(int32_t type, int32_t material, const float* a, const float* b,
+                       const float* cc, float s0, float s1, pgpu_prim* out) {
+    if (!out) return PGPU_ERR_INVALID_ARG;
+    return make_prim(type, material, a, b, cc, s0, s1, out);
+}
+
+int32_t pgpu_build_bvh(const pgpu_scene* s, pgpu_bvh_node* out_nodes, int32_t* out_n_nodes,
+                       int32_t* out_depth) {
+    if (!s || !out_n_nodes || (s->n_prims > 0 && !s->prims) || s->n_prims < 0 ||
+        s->n_mesh_triangles < 0 ||
+        (s->n_mesh_triangles > 0 && (!s->mesh_indices || !s->mesh_vertices)))
+        return PGPU_ERR_INVALID_ARG;
+    for (int k = 0; k < 3 * s->n_mesh_triangles; ++k)
+        if (s->mesh_indices[k] < 0 || s->mesh_indices[k] >= s->n_mesh_vertices)
+            return PGPU_ERR_INVALID_ARG;
+    std::vector<pgpu_prim> prims;
+    unified_prims(*s, prims);
+    std::vector<pgpu_bvh_node> nodes;
+    int depth = 0;
+    build_bvh(prims, nodes, depth);
+    if (out_nodes) std::memcpy(out_nodes, nodes.data(), nodes.size() * sizeof(pgpu_bvh_node));
+    *out_n_nodes = (int32_t)nodes.size();
+    if (out_depth) *out_depth = depth;
+    return PGPU_OK;
+}
+
+int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    if (!s || !out_id) return fail(c, PGPU_ERR_INVALID_ARG, "null scene or id pointer");
+    if (s->n_prims < 0 || s->n_mesh_triangles < 0 || s->n_materials < 0 || s->n_lights < 0 ||
+        s->n_nodes < 0 || s->n_mesh_vertices < 0)
+        return fail(c, PGPU_ERR_INVALID_ARG, "negative count");
+    if ((s->n_prims && !s->prims) || (s->n_materials && !s->materials) ||
+        (s->n_lights && !s->lights) ||
+        (s->n_mesh_triangles && (!s->mesh_indices || !s->mesh_vertices || !s->mesh_materials)))
+        return fail(c, PGPU_ERR_INVALID_ARG, "null array with a nonzero count");
+    if (s->camera.aperture != 0.0f)
+        return fail(c, PGPU_ERR_UNSUPPORTED, "camera aperture (depth of field) is not supported");
+    const long long n_unified = (long long)s->n_prims + s->n_mesh_triangles;
+    if (n_unified >= kMaxLeaves) return fail(c, PGPU_ERR_UNSUPPORTED, "too many primitives");
+    const int nU = (int)n_unified;
+    for (int k = 0; k < s->n_prims; ++k) {
+        int rc = check_prim(c, s->prims[k], k, s->n_materials);
+        if (rc) return rc;
+    }
+    for (int k = 0; k < s->n_mesh_triangles; ++k) {
+        for (int v = 0; v < 3; ++v) {
+            int idx = s->mesh_indices[3 * k + v];
+            if (idx < 0 || idx >= s->n_mesh_vertices)
+                return fail(c, PGPU_ERR_INVALID_ARG, "mesh triangle %d vertex %d out of range", k, idx);
+        }
+        if (s->mesh_materials[k] < 0 || s->mesh_materials[k] >= s->n_materials)
+            return fail(c, PGPU_ERR_INVALID_ARG, "mesh triangle %d material out of range", k);
+    }
+    for (int k = 0; k < s->n_mesh_vertices; ++k)
+        if (!finite3(s->mesh_vertices + 3 * k))
+            return fail(c, PGPU_ERR_INVALID_ARG, "mesh vertex %d is not finite", k);
+    std::vector<DevMaterial> mats(s->n_materials);
+    for (int k = 0; k < s->n_materials; ++k) {
+        const pgpu_material& m = s->materials[k];
+        if (m.kind < PGPU_MAT_DIFFUSE || m.kind > PGPU_MAT_DIELECTRIC)
+            return fail(c, PGPU_ERR_UNSUPPORTED, "material %d has unsupported kind %d", k, m.kind);
+        if (m.flags != 0) return fail(c, PGPU_ERR_UNSUPPORTED, "material %d has flags set", k);
+        DevMaterial d{};
+        std::memcpy(d.albedo, m.albedo, 12);
+        d.kind = m.kind;
+        std::memcpy(d.emission, m.emission, 12);
+        d.reflectivity = m.reflectivity;
+        d.ior = m.ior;
+        d.specular = m.specular;
+        d.shininess = m.shininess;
+        std::memcpy(d.specular_color, m.specular_color, 12);
+        mats[k] = d;
+    }
+    std::vector<DevLight> lights(s->n_lights);
+    std::vector<int> quad_mats;
+    int has_quad = 0;
+    for (int k = 0; k < s->n_lights; ++k) {
+        const pgpu_light& l = s->lights[k];
+        if (l.kind < PGPU_LIGHT_POINT || l.kind > PGPU_LIGHT_QUAD)
+            return fail(c, PGPU_ERR_UNSUPPORTED, "light %d has unsupported kind %d", k, l.kind);
+        DevLight d{};
+        d.kind = l.kind;
+        std::memcpy(d.pos, l.pos, 12);
+        std::memcpy(d.intensity, l.intensity, 12);
+        d.radius = l.radius;
+        d.is_emissive = l.is_emissive;
+        std::memcpy(d.edge_u, l.edge_u, 12);
+        std::memcpy(d.edge_v, l.edge_v, 12);
+        if (l.kind == PGPU_LIGHT_QUAD) {
+            if (l.material < 0 || l.material >= s->n_materials)
+                return fail(c, PGPU_ERR_INVALID_ARG, "quad light %d material out of range", k);
+            HV cr = hcross(hv(l.edge_u), hv(l.edge_v));
+            d.area = std::sqrt(cr.x * cr.x + cr.y * cr.y + cr.z * cr.z);
+            if (!(d.area > 0.0f)) return fail(c, PGPU_ERR_INVALID_ARG, "quad light %d has no area", k);
+            mats[l.material].area_emitter = 1;
+            quad_mats.push_back(l.material);
+            has_quad = 1;
+        }
+        lights[k] = d;
+    }
+
+    // BVH: caller's table (Pencil's tree) or the same tree built here
+    std::vector<pgpu_prim> prims;
+    unified_prims(*s, prims);
+    std::vector<pgpu_bvh_node> built;
+    const pgpu_bvh_node* nodes = s->nodes;
+    int n_nodes = s->n_nodes;
+    int depth = 0;
+    if (!nodes) {
+        build_bvh(prims, built, depth);
+        nodes = built.data();
+        n_nodes = (int)built.size();
+    }
+    int rc = check_tree(c, nodes, n_nodes, nU, depth);
+    if (rc) return rc;
+
+    // DFS order numbering: interior nodes and leaf slots
+    std::vector<int> idx(n_nodes);
+    int n_int = 0, n_leaf = 0;
+    for (int k = 0; k < n_nodes; ++k) idx[k] = nodes[k].left < 0 ? n_leaf++ : n_int++;
+    // vertices: mesh vertices first, then those of explicit triangles
+    int n_explicit_tri = 0;
+    for (int k = 0; k < s->n_prims; ++k) n_explicit_tri += s->prims[k].type == PGPU_PRIM_TRIANGLE;
+    const size_t n_verts = (size_t)s->n_mesh_vertices + 3 * (size_t)n_explicit_tri;
+
+    size_t off_nodes = 0;
+    size_t off_ga = align256(off_nodes + (size_t)n_int * 64);
+    size_t off_gb = align256(off_ga + (size_t)n_leaf * 16);
+    size_t off_vt = align256(off_gb + (size_t)n_leaf * 16);
+    size_t off_lm = align256(off_vt + n_verts * 16);
+    size_t off_lp = align256(off_lm + (size_t)n_leaf * 4);
+    size_t off_mt = align256(off_lp + (size_t)n_leaf * 4);
+    size_t off_lt = align256(off_mt + mats.size() * sizeof(DevMaterial));
+    size_t total = align256(off_lt + lights.size() * sizeof(DevLight));
+    std::vector<unsigned char> host(total, 0);
+    float4* h_nodes = reinterpret_cast<float4*>(host.data() + off_nodes);
+    float4* h_ga = reinterpret_cast<float4*>(host.data() + off_ga);
+    float4* h_gb = reinterpret_cast<float4*>(host.data() + off_gb);
+    float4* h_vt = reinterpret_cast<float4*>(host.data() + off_vt);
+    int* h_lm = reinterpret_cast<int*>(host.data() + off_lm);
+    int* h_lp = reinterpret_cast<int*>(host.data() + off_lp);
+    for (int k = 0; k < s->n_mesh_vertices; ++k)
+        h_vt[k] = make_float4(s->mesh_vertices[3 * k], s->mesh_vertices[3 * k + 1],
+                              s->mesh_vertices[3 * k + 2], 0.0f);
+    size_t next_vert = (size_t)s->n_mesh_vertices;
+
+    auto ref_of = [&](int k) -> int {
+        if (nodes[k].left >= 0) return idx[k];
+        int prim = nodes[k].right;
+        int type = prim < s->n_prims ? s->prims[prim].type : PGPU_PRIM_TRIANGLE;
+        return ~((type << kLeafTypeShift) | idx[k]);
+    };
+    for (int k = 0; k < n_nodes; ++k) {
+        const pgpu_bvh_node& nd = nodes[k];
+        if (nd.left >= 0) {
+            const pgpu_bvh_node& L = nodes[nd.left];
+            const pgpu_bvh_node& R = nodes[nd.right];
+            float4* q = h_nodes + 4 * (size_t)idx[k];
+            q[0] = make_float4(L.bmin[0], L.bmin[1], L.bmin[2], L.bmax[0]);
+            q[1] = make_float4(L.bmax[1], L.bmax[2], R.bmin[0], R.bmin[1]);
+            q[2] = make_float4(R.bmin[2], R.bmax[0], R.bmax[1], R.bmax[2]);
+            int4 refs = make_int4(ref_of(nd.left), ref_of(nd.right), 0, 0);
+            std::memcpy(&q[3], &refs, 16);
+            continue;
+        }
+        const int slot = idx[k];
+        const int prim = nd.right;
+        h_lp[slot] = prim;
+        if (prim >= s->n_prims) {
+            int t = prim - s->n_prims;
+            h_lm[slot] = s->mesh_materials[t];
+            int4 tri = make_int4(s->mesh_indices[3 * t], s->mesh_indices[3 * t + 1],
+                                 s->mesh_indices[3 * t + 2], 0);
+            std::memcpy(&h_ga[slot], &tri, 16);
+            continue;
+        }
+        const pgpu_prim& p = s->prims[prim];
+        const float* q = p.p;
+        h_lm[slot] = p.material;
+        switch (p.type) {
+            case PGPU_PRIM_SPHERE:
+            case PGPU_PRIM_CUBE:
+                h_ga[slot] = make_float4(q[0], q[1], q[2], q[3]);
+                break;
+            case PGPU_PRIM_TRIANGLE: {
+                int base = (int)next_vert;
+                for (int v = 0; v < 3; ++v)
+                    h_vt[next_vert++] = make_float4(q[3 * v], q[3 * v + 1], q[3 * v + 2], 0.0f);
+                int4 tri = make_int4(base, base + 1, base + 2, 0);
+                std::memcpy(&h_ga[slot], &tri, 16);
+                break;
+            }
+            case PGPU_PRIM_PLANE:
+                h_ga[slot] = make_float4(q[0], q[1], q[2], 0.0f);
+                h_gb[slot] = make_float4(q[3], q[4], q[5], 0.0f);
+                break;
+            case PGPU_PRIM_CYLINDER:
+            case PGPU_PRIM_CONE:
+                h_ga[slot] = make_float4(q[0], q[1], q[2], q[6]);
+                h_gb[slot] = make_float4(q[3], q[4], q[5], q[7]);
+                break;
+        }
+    }
+    std::memcpy(host.data() + off_mt, mats.data(), mats.size() * sizeof(DevMaterial));
+    std::memcpy(host.data() + off_lt, lights.data(), lights.size() * sizeof(DevLight));
+
+    PGPU_CUDA(c, cudaSetDevice(c->device));
+    auto ds = std::make_unique<DeviceScene>();
+    cudaError_t e = cudaMalloc(&ds->arena, total);
+    if (e != cudaSuccess)
+        return fail(c, PGPU_ERR_OUT_OF_MEMORY, "scene arena of %zu bytes: %s", total,
+                    cudaGetErrorString(e));
+    ds->bytes = total;
+    e = cudaMemcpyAsync(ds->arena, host.data(), total, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        cudaFree(ds->arena);
+        return cuda_fail(c, e, "scene upload");
+    }
+    unsigned char* base = static_cast<unsigned char*>(ds->arena);
+    SceneView& v = ds->view;
+    v.nodes = reinterpret_cast<const float4*>(base + off_nodes);
+    v.geo_a = reinterpret_cast<const float4*>(base + off_ga);
+    v.geo_b = reinterpret_cast<const float4*>(base + off_gb);
+    v.verts = reinterpret_cast<const float4*>(base + off_vt);
+    v.leaf_mat = reinterpret_cast<const int*>(base + off_lm);
+    v.leaf_prim = reinterpret_cast<const int*>(base + off_lp);
+    v.mats = reinterpret_cast<const DevMaterial*>(base + off_mt);
+    v.lights = reinterpret_cast<const DevLight*>(base + off_lt);
+    v.n_lights = s->n_lights;
+    v.n_leaves = n_leaf;
+    v.has_quad_lights = has_quad;
+    if (n_nodes == 0) {
+        v.root_ref = kEmptyRoot;
+    } else {
+        v.root_ref = ref_of(0);
+        std::memcpy(v.root_min, nodes[0].bmin, 12);
+        std::memcpy(v.root_max, nodes[0].bmax, 12);
+    }
+    camera_basis(s->camera, v.cam);
+    std::memcpy(v.bg, s->background, 12);
+    std::memcpy(v.amb, s->ambient, 12);
+    ds->n_unified = nU;
+    ds->n_leaves = n_leaf;
+    ds->depth = depth;
+    ds->mats = mats;
+    ds->lights = lights;
+    ds->quad_mats = quad_mats;
+    ds->d_mats = reinterpret_cast<DevMaterial*>(base + off_mt);
+    int id = c->next_id++;
+    c->scenes[id] = std::move(ds);
+    *out_id = id;
+    return PGPU_OK;
+}
+
+int32_t pgpu_free_scene(pgpu_ctx* c, int32_t id) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    DeviceScene* ds = find_scene(c, id);
+    if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(ds->arena);
+    c->scenes.erase(id);
+    return PGPU_OK;
+}
+
+int32_t pgpu_update_materials(pgpu_ctx* c, int32_t id, const pgpu_material* m, int32_t n) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    DeviceScene* ds = find_scene(c, id);
+    if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
+    if (!m || n != (int)ds->mats.size())
+        return fail(c, PGPU_ERR_INVALID_ARG, "material count %d, scene has %zu", n, ds->mats.size());
+    std::vector<DevMaterial> mats(ds->mats);
+    for (int k = 0; k < n; ++k) {
+        if (m[k].kind < PGPU_MAT_DIFFUSE || m[k].kind > PGPU_MAT_DIELECTRIC || m[k].flags != 0)
+            return fail(c, PGPU_ERR_UNSUPPORTED, "material %d unsupported", k);
+        DevMaterial& d = mats[k];
+        std::memcpy(d.albedo, m[k].albedo, 12);
+        d.kind = m[k].kind;
+        std::memcpy(d.emission, m[k].emission, 12);
+        d.reflectivity = m[k].reflectivity;
+        d.ior = m[k].ior;
+        d.specular = m[k].specular;
+        d.shininess = m[k].shininess;
+        std::memcpy(d.specular_color, m[k].specular_color, 12);
+    }
+    PGPU_CUDA(c, cudaMemcpyAsync(ds->d_mats, mats.data(), mats.size() * sizeof(DevMaterial),
+                                 cudaMemcpyHostToDevice, c->stream));
+    PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    ds->mats = mats;
+    return PGPU_OK;
+}
+
+}  // extern "C"
+
+namespace pgpu {
+
+// Validate render parameters; fills cfg.
+int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, RenderCfg& cfg) {
+    if (!p) return fail(c, PGPU_ERR_INVALID_ARG, "null render params");
+    if (p->width <= 0 || p->height <= 0 || p->samples <= 0 || p->depth < 0)
+        return fail(c, PGPU_ERR_INVALID_ARG, "bad size %dx%d, samples %d, depth %d", p->width,
+                    p->height, p->samples, p->depth);
+    if ((long long)p->width * p->height > (1LL << 28) || p->samples > 64)
+        return fail(c, PGPU_ERR_INVALID_ARG, "image of %dx%d with n=%d is too large", p->width,
+                    p->height, p->samples);
+    if (p->mode != PGPU_MODE_PATHTRACE && p->mode != PGPU_MODE_WHITTED)
+        return fail(c, PGPU_ERR_INVALID_ARG, "unknown mode %d", p->mode);
+    if (p->engine != PGPU_ENGINE_WAVEFRONT && p->engine != PGPU_ENGINE_MEGAKERNEL)
+        return fail(c, PGPU_ERR_INVALID_ARG, "unknown engine %d", p->engine);
+    if (p->rng != PGPU_RNG_COUNTER && p->rng != PGPU_RNG_PIXEL_SEQUENTIAL)
+        return fail(c, PGPU_ERR_INVALID_ARG, "unknown rng %d", p->rng);
+    if (p->glass != PGPU_GLASS_FRESNEL_SPLIT && p->glass != PGPU_GLASS_BOTH_BRANCHES)
+        return fail(c, PGPU_ERR_INVALID_ARG, "unknown glass mode %d", p->glass);
+    if (!(p->shadow_bias >= 0.0f) || p->soft_shadow_samples <= 0 || p->sample_offset < 0)
+        return fail(c, PGPU_ERR_INVALID_ARG, "bad shadow bias, soft-shadow samples or offset");
+    if (p->engine == PGPU_ENGINE_WAVEFRONT &&
+        (p->rng != PGPU_RNG_COUNTER || p->glass != PGPU_GLASS_FRESNEL_SPLIT))
+        return fail(c, PGPU_ERR_UNSUPPORTED,
+                    "the wavefront engine needs the counter RNG and Fresnel-split glass");
+    if (p->glass == PGPU_GLASS_BOTH_BRANCHES && p->depth > kMaxTreeFrames)
+        return fail(c, PGPU_ERR_UNSUPPORTED, "two-branch glass supports depth <= %d", kMaxTreeFrames);
+    cfg.W = p->width;
+    cfg.H = p->height;
+    cfg.n = p->samples;
+    cfg.spp = p->samples * p->samples;
+    cfg.depth = p->depth;
+    cfg.mode = p->mode;
+    cfg.engine = p->engine;
+    cfg.rng = p->rng;
+    cfg.glass = p->glass;
+    cfg.soft = p->soft_shadow_samples;
+    cfg.bias = p->shadow_bias;
+    cfg.salt = p->seed;
+    cfg.sample_offset = p->sample_offset;
+    cfg.count = (p->flags & (PGPU_FLAG_COUNT_RAYS | PGPU_FLAG_COUNT_NODES)) != 0;
+    cfg.block = p->block_size;
+    cfg.queue_capacity = p->queue_capacity;
+    cfg.sort_key = p->sort_key;
+    (void)ds;
+    return PGPU_OK;
+}
+
+// Run jobs through the wavefront engine; checks the device status word.
+int run_wavefront(pgpu_ctx* c, const std::vector<DeviceScene*>& scenes,
+                  const std::vector<RenderCfg>& cfgs, const std::vector<float*>& outs,
+                  const std::vector<float*>& m2s, bool use_graph, int* launches) {
+    std::vector<SceneView> views;
+    std::vector<std::vector<DevLight>> lights;
+    std::vector<int> job_view;
+    std::map<const DeviceScene*, int> vidx;
+    for (auto* ds : scenes) {
+        auto it = vidx.find(ds);
+        if (it == vidx.end()) {
+            int k = (int)views.size();
+            vidx[ds] = k;
+            views.push_back(ds->view);
+            lights.push_back(ds->lights);
+            job_view.push_back(k);
+        } else {
+            job_view.push_back(it->second);
+        }
+    }
+    *c->h_status = 0;
+    cudaError_t e = wavefront_render(*c->wf, views, lights, job_view, cfgs, outs, m2s, c->d_cnt,
+                                     c->stream, use_graph, launches, c->h_status);
+    if (e != cudaSuccess) return cuda_fail(c, e, "wavefront launch");
+    return PGPU_OK;
+}
+
+}  // namespace pgpu
+
+extern "C" {
+
+int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float* out_rgb,
+                    float* out_m2, pgpu_stats* stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    DeviceScene* ds = find_scene(c, id);
+    if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
+    if (!out_rgb) return fail(c, PGPU_ERR_INVALID_ARG, "null output");
+    RenderCfg cfg;
+    int rc = make_cfg(c, ds, p, cfg);
+    if (rc) return rc;
+    PGPU_CUDA(c, cudaSetDevice(c->device));
+    const bool dev_out = (p->flags & PGPU_FLAG_DEVICE_OUTPUT) != 0;
+    const size_t n3 = (size_t)cfg.W * cfg.H * 3;
+    float* d_out = dev_out ? out_rgb : nullptr;
+    float* d_m2 = dev_out ? out_m2 : nullptr;
+    if (!dev_out) {
+        if ((rc = ensure(c, c->d_out, c->out_cap, n3 * 4))) return rc;
+        d_out = c->d_out;
+        if (out_m2) {
+            if ((rc = ensure(c, c->d_m2, c->m2_cap, n3 * 4))) return rc;
+            d_m2 = c->d_m2;
+        }
+    }
+    if (cfg.count)
+        PGPU_CUDA(c, cudaMemsetAsync(c->d_cnt, 0, CNT_N * sizeof(unsigned long long), c->stream));
+    int launches = 1;
+    PGPU_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    cudaError_t e;
+    if (cfg.engine == PGPU_ENGINE_MEGAKERNEL) {
+        e = launch_megakernel(ds->view, cfg, d_out, d_m2, c->d_cnt, c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "megakernel launch");
+    } else {
+        *c->h_status = 0;
+        rc = run_wavefront(c, {ds}, {cfg}, {d_out}, {d_m2}, (p->flags & PGPU_FLAG_NO_GRAPH) == 0,
+                           &launches);
+        if (rc) return rc;
+    }
+    PGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    if (!dev_out) {
+        PGPU_CUDA(c, cudaMemcpyAsync(out_rgb, d_out, n3 * 4, cudaMemcpyDeviceToHost, c->stream));
+        if (out_m2)
+            PGPU_CUDA(c, cudaMemcpyAsync(out_m2, d_m2, n3 * 4, cudaMemcpyDeviceToHost, c->stream));
+    }
+    unsigned long long cnt[CNT_N] = {0};
+    if (cfg.count)
+        PGPU_CUDA(c, cudaMemcpyAsync(cnt, c->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+    PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (cfg.engine == PGPU_ENGINE_WAVEFRONT && *c->h_status != 0)
+        return fail(c, PGPU_ERR_QUEUE_OVERFLOW, "shadow record queue overflow");
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        stats->device_ms = ms;
+        stats->paths = (uint64_t)cfg.W * cfg.H * cfg.spp;
+        stats->extension_rays = cnt[CNT_EXT];
+        stats->shadow_rays = cnt[CNT_SHADOW];
+        stats->reference_rays = cnt[CNT_REF];
+        stats->node_visits = cnt[CNT_NODES];
+        stats->prim_tests = cnt[CNT_PRIMS];
+        stats->kernel_launches = launches;
+        stats->total_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return PGPU_OK;
+}
+
+int32_t pgpu_render_batch(pgpu_ctx* c, int32_t n_jobs, const int32_t* ids,
+                          const pgpu_render_params* params, float* const* outs, pgpu_stats* stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    if (n_jobs <= 0 || !ids || !params || !outs)
+        return fail(c, PGPU_ERR_INVALID_ARG, "bad batch arguments");
+    std::vector<DeviceScene*> scenes(n_jobs);
+    std::vector<RenderCfg> cfgs(n_jobs);
+    size_t total = 0;
+    bool dev_out = (params[0].flags & PGPU_FLAG_DEVICE_OUTPUT) != 0;
+    for (int k = 0; k < n_jobs; ++k) {
+        scenes[k] = find_scene(c, ids[k]);
+        if (!scenes[k]) return fail(c, PGPU_ERR_NO_SCENE, "job %d: unknown scene id %d", k, ids[k]);
+        int rc = make_cfg(c, scenes[k], &params[k], cfgs[k]);
+        if (rc) return rc;
+        if (cfgs[k].engine != PGPU_ENGINE_WAVEFRONT)
+            return fail(c, PGPU_ERR_UNSUPPORTED, "job %d: batches run on the wavefront engine", k);
+        if (((params[k].flags & PGPU_FLAG_DEVICE_OUTPUT) != 0) != dev_out)
+            return fail(c, PGPU_ERR_INVALID_ARG, "jobs mix host and device outputs");
+        if (!outs[k]) return fail(c, PGPU_ERR_INVALID_ARG, "job %d: null output", k);
+        total += (size_t)cfgs[k].W * cfgs[k].H * 3;
+    }
+    PGPU_CUDA(c, cudaSetDevice(c->device));
+    std::vector<float*> d_outs(n_jobs), d_m2s(n_jobs, nullptr);
+    if (dev_out) {
+        for (int k = 0; k < n_jobs; ++k) d_outs[k] = outs[k];
+    } else {
+        int rc = ensure(c, c->d_out, c->out_cap, total * 4);
+        if (rc) return rc;
+        size_t off = 0;
+        for (int k = 0; k < n_jobs; ++k) {
+            d_outs[k] = c->d_out + off;
+            off += (size_t)cfgs[k].W * cfgs[k].H * 3;
+        }
+    }
+    bool count = false;
+    for (auto& cf : cfgs) count = count || cf.count;
+    if (count) PGPU_CUDA(c, cudaMemsetAsync(c->d_cnt, 0, CNT_N * sizeof(unsigned long long), c->stream));
+    int launches = 0;
+    PGPU_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    int rc = run_wavefront(c, scenes, cfgs, d_outs, d_m2s, (params[0].flags & PGPU_FLAG_NO_GRAPH) == 0,
+                           &launches);
+    if (rc) return rc;
+    PGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    if (!dev_out)
+        for (int k = 0; k < n_jobs; ++k)
+            PGPU_CUDA(c, cudaMemcpyAsync(outs[k], d_outs[k], (size_t)cfgs[k].W * cfgs[k].H * 12,
+                                         cudaMemcpyDeviceToHost, c->stream));
+    unsigned long long cnt[CNT_N] = {0};
+    if (count)
+        PGPU_CUDA(c, cudaMemcpyAsync(cnt, c->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+    PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (*c->h_status != 0) return fail(c, PGPU_ERR_QUEUE_OVERFLOW, "shadow record queue overflow");
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        stats->device_ms = ms;
+        for (auto& cf : cfgs) stats->paths += (uint64_t)cf.W * cf.H * cf.spp;
+        stats->extension_rays = cnt[CNT_EXT];
+        stats->shadow_rays = cnt[CNT_SHADOW];
+        stats->reference_rays = cnt[CNT_REF];
+        stats->node_visits = cnt[CNT_NODES];
+        stats->prim_tests = cnt[CNT_PRIMS];
+        stats->kernel_launches = launches;
+        stats->total_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return PGPU_OK;
+}
+
+int32_t pgpu_adjoint(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, const float* dl,
+                     double* d_albedo, double* d_emission, double* d_light, float* out_rgb,
+                     pgpu_stats* stats) {
+    (void)id; (void)p; (void)dl; (void)d_albedo; (void)d_emission; (void)d_light; (void)out_rgb;
+    (void)stats;
+    return fail(c, PGPU_ERR_UNSUPPORTED, "adjoint not built yet");
+}
+
+static int32_t run_query(pgpu_ctx* c, int32_t id, bool camera, const float* in, int32_t n,
+                         int32_t* prim, float* t) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    DeviceScene* ds = find_scene(c, id);
+    if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
+    if (n < 0 || (n > 0 && (!in || !prim || !t))) return fail(c, PGPU_ERR_INVALID_ARG, "bad query");
+    if (n == 0) return PGPU_OK;
+    PGPU_CUDA(c, cudaSetDevice(c->device));
+    const size_t in_b = (size_t)n * (camera ? 2 : 6) * 4;
+    const size_t need = align256(in_b) + 2 * align256((size_t)n * 4);
+    int rc = ensure(c, reinterpret_cast<unsigned char*&>(c->d_query), c->query_cap, need);
+    if (rc) return rc;
+    unsigned char* b = static_cast<unsigned char*>(c->d_query);
+    float* d_in = reinterpret_cast<float*>(b);
+    int* d_prim = reinterpret_cast<int*>(b + align256(in_b));
+    float* d_t = reinterpret_cast<float*>(b + align256(in_b) + align256((size_t)n * 4));
+    PGPU_CUDA(c, cudaMemcpyAsync(d_in, in, in_b, cudaMemcpyHostToDevice, c->stream));
+    cudaError_t e = launch_query(ds->view, camera, d_in, n, d_prim, d_t, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "query launch");
+    PGPU_CUDA(c, cudaMemcpyAsync(prim, d_prim, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    PGPU_CUDA(c, cudaMemcpyAsync(t, d_t, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+int32_t pgpu_trace_rays(pgpu_ctx* c, int32_t id, const float* rays, int32_t n, int32_t* prim,
+                        float* t) {
+    return run_query(c, id, false, rays, n, prim, t);
+}
+
+int32_t pgpu_primary_hits(pgpu_ctx* c, int32_t id, const float* uv, int32_t n, int32_t* prim,
+                          float* t) {
+    return run_query(c, id, true, uv, n, prim, t);
+}
+
+}  // extern "C"

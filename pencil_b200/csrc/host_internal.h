@@ -1,0 +1,43 @@
+// host_internal.h - declarations shared by the host-side translation units
+// of libpencil_gpu.so.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/pencil_gpu.h"
+#include "scene_layout.h"
+
+namespace pgpu {
+
+// bvh_build.cpp
+void unified_prims(const pgpu_scene& s, std::vector<pgpu_prim>& out);
+void build_bvh(const std::vector<pgpu_prim>& prims, std::vector<pgpu_bvh_node>& nodes,
+               int& depth);
+int make_prim(int type, int material, const float* a, const float* b, const float* c, float s0,
+              float s1, pgpu_prim* out);
+
+// Render configuration after validation.
+struct RenderCfg {
+    int W, H, n, spp, depth, mode, engine, rng, glass, soft;
+    float bias;
+    uint32_t salt;
+    int sample_offset;
+    bool count;
+    int block;
+    int queue_capacity;
+    int sort_key;
+};
+
+// Device counters written by the kernels (atomic adds).
+enum DevCounter {
+    CNT_EXT = 0,
+    CNT_SHADOW = 1,
+    CNT_REF = 2,
+    CNT_NODES = 3,
+    CNT_LEAF_BYTES = 4,
+    CNT_PRIMS = 5,
+    CNT_N = 8
+};
+
+}  // namespace pgpu

@@ -1,0 +1,701 @@
+// wavefront.cu - the wavefront path tracer.
+//
+// Paths of one or many render jobs (scenes of uneven size) form one path
+// space: job after job, pixel after pixel, sample after sample. The space is
+// processed in chunks of whole pixels that fit the queue capacity Q. For each
+// chunk the kernels run
+//
+//   generate                          camera rays of every path in the chunk
+//   depth x { extend, shade, shadow } closest hit / shade_vertex / any hit
+//   accumulate                        per-pixel sums in the megakernel's order
+//
+// extend, shade and shadow are persistent: a grid sized to fill the GPU whose
+// warps fetch 32 queue entries at a time from an atomic cursor. Path state
+// lives in SoA arrays indexed by the path's slot in the chunk (float4 fields,
+// so every access is one coalesced 128-bit load); queues hold slots. shade
+// compacts surviving paths into the next queue with one atomic per warp
+// (ballot + popc), optionally binned by the octant of the new ray direction
+// (sort key 1) so that warps traverse with matching near/far child order.
+// Next-event shadow rays are stored per slot and resolved by shadow in the
+// order shade made them, with the same NeeAccum as the megakernel, so each
+// path's radiance is bit-identical to the megakernel's. The whole frame is
+// one CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "host_internal.h"
+#include "path.cuh"
+
+namespace pgpu {
+
+constexpr int kWfShared = 16;
+constexpr int kWfBlock = 128;
+constexpr int kOctants = 8;
+
+// One render job of the path space.
+struct WfJob {
+    PathParams P;
+    int view;                 // index into the SceneView table
+    long long path_off;       // first path of the job in the path space
+    long long pix_off;        // first pixel of the job in the pixel space
+    int G;                    // accumulation lanes (as the megakernel's)
+    float* out;               // device image
+    float* m2;                // device second moments (or null)
+};
+
+// Device buffers of the wavefront (capacity Q slots, S shadow records each).
+struct WfArgs {
+    const SceneView* views;
+    const WfJob* jobs;
+    int n_jobs;
+    int Q;
+    int maxS;
+    float4* ray_o;
+    float4* ray_d;
+    float4* T;
+    float4* L;
+    uint4* st;                // rng, depth, flags, job
+    float4* hit;              // t, best ref, leaf slot, found
+    float4* pb;               // pending base.xyz, record count
+    float4* pt;               // pending tail.xyz, scale s
+    float4* pw;               // pending weight.xyz, kind
+    float4* sh_o;             // [k * Q + slot] origin.xyz, tmin
+    float4* sh_d;             // direction.xyz, tmax
+    float4* sh_c;             // contribution.xyz, test | group_end << 1
+    int* q[2];                // queues: kOctants bins of Q entries each
+    int* counts;              // [iteration * kOctants + bin]
+    unsigned int* work;       // [iteration * 3 + kernel] fetch cursors
+    int* status;              // 1: shadow record overflow
+    unsigned long long* counters;
+    int sort_key;
+};
+
+__device__ __forceinline__ int find_job(const WfJob* jobs, int n, long long path) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].path_off <= path) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int find_job_pix(const WfJob* jobs, int n, long long pix) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].pix_off <= pix) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ void flush_counts(const WfArgs& A, const RayCount& rc) {
+    if (!COUNT) return;
+    unsigned long long v[6] = {rc.ext, rc.shadow, rc.ref, rc.tc.nodes, rc.tc.leaf_bytes,
+                               rc.tc.prims};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        unsigned long long x = v[k];
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+        if ((threadIdx.x & 31) == 0 && x) atomicAdd(A.counters + k, x);
+    }
+}
+
+// Number of entries in iteration `it`'s queue and the queue entry -> slot map
+// across octant bins.
+struct QView {
+    const int* q;
+    int Q;
+    int cnt[kOctants];
+    int total;
+    __device__ __forceinline__ int slot(int e) const {
+        int b = 0;
+#pragma unroll
+        for (int k = 0; k < kOctants - 1; ++k) {
+            if (e >= cnt[b]) { e -= cnt[b]; ++b; }
+        }
+        return q[b * Q + e];
+    }
+};
+__device__ __forceinline__ QView qview(const WfArgs& A, int it) {
+    QView v;
+    v.q = A.q[it & 1];
+    v.Q = A.Q;
+    v.total = 0;
+#pragma unroll
+    for (int k = 0; k < kOctants; ++k) {
+        v.cnt[k] = A.counts[it * kOctants + k];
+        v.total += v.cnt[k];
+    }
+    return v;
+}
+
+// Warp-cooperative fetch of 32 queue entries; returns the base (>= total: done).
+__device__ __forceinline__ int fetch32(unsigned int* cursor) {
+    int base = 0;
+    if ((threadIdx.x & 31) == 0) base = (int)atomicAdd(cursor, 32u);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+
+// ---- generate -----------------------------------------------------------------
+template <bool COUNT>
+__global__ void __launch_bounds__(kWfBlock)
+wf_generate(WfArgs A, long long path_begin, int n_slots) {
+    RayCount rc = {};
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    bool live = false;
+    if (slot < n_slots) {
+        long long path = path_begin + slot;
+        int jb = find_job(A.jobs, A.n_jobs, path);
+        const WfJob& J = A.jobs[jb];
+        const PathParams& P = J.P;
+        const SceneView& S = A.views[J.view];
+        long long local = path - J.path_off;
+        int pix = (int)(local / P.spp);
+        int s = (int)(local % P.spp);
+        int i = pix % P.W, j = pix / P.W;
+        Rng rng{path_seed(i, j, s + P.sample_offset, P.salt)};
+        float u, v;
+        sample_uv(i, j, s % P.n, s / P.n, P.W, P.H, P.n, rng, u, v);
+        Ray r = camera_ray(S.cam, u, v);
+        A.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
+        A.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
+        A.T[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        A.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        A.pw[slot] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
+        uint32_t flags = P.mode == kModeWhitted ? kFlagWhitted : 0u;
+        A.st[slot] = make_uint4(rng.s, (unsigned)P.depth, flags, (unsigned)jb);
+        if (COUNT) rc.ref++;
+        live = P.depth > 0;
+    }
+    unsigned m = __ballot_sync(0xffffffffu, live);
+    if (m) {
+        int first = 0;
+        if (lane == __ffs(m) - 1) first = atomicAdd(A.counts, __popc(m));
+        first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
+        if (live) A.q[0][first + __popc(m & ((1u << lane) - 1u))] = slot;
+    }
+    flush_counts<COUNT>(A, rc);
+}
+
+// ---- extend -------------------------------------------------------------------
+template <bool COUNT>
+__global__ void __launch_bounds__(kWfBlock)
+wf_extend(WfArgs A, int it) {
+    extern __shared__ int smem[];
+    TravStack<kWfShared> stk;
+    stk.sref = smem + threadIdx.x;
+    stk.st = reinterpret_cast<float*>(smem + kWfShared * blockDim.x) + threadIdx.x;
+    stk.stride = blockDim.x;
+    RayCount rc = {};
+    QView qv = qview(A, it);
+    unsigned int* cursor = A.work + it * 3 + 0;
+    while (true) {
+        int base = fetch32(cursor);
+        if (base >= qv.total) break;
+        int e = base + (threadIdx.x & 31);
+        if (e < qv.total) {
+            int slot = qv.slot(e);
+            int jb = (int)A.st[slot].w;
+            const SceneView& S = A.views[A.jobs[jb].view];
+            float4 o = A.ray_o[slot], d = A.ray_d[slot];
+            Ray r{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)};
+            if (COUNT) rc.ext++;
+            float tb;
+            int bref;
+            int leaf = closest_hit<kWfShared, COUNT>(S, r, 1e-4f, 1e9f, tb, bref, stk, &rc.tc);
+            A.hit[slot] = make_float4(tb, __int_as_float(bref), __int_as_float(leaf), 0.0f);
+        }
+    }
+    flush_counts<COUNT>(A, rc);
+}
+
+// ---- shade --------------------------------------------------------------------
+// Emitter that stores a vertex's shadow records and pending terms per slot.
+struct StoreNee {
+    const WfArgs& A;
+    int slot;
+    int n;
+    int kind;
+    V3 base, tail, w;
+    float s;
+    __device__ StoreNee(const WfArgs& a, int sl)
+        : A(a), slot(sl), n(0), kind(0), base(v3(0, 0, 0)), tail(v3(0, 0, 0)), w(v3(0, 0, 0)),
+          s(0.0f) {}
+    __device__ __forceinline__ void begin_none() { kind = 0; }
+    __device__ __forceinline__ void begin_pt() { kind = 1; }
+    __device__ __forceinline__ void begin_whitted(V3 b) { kind = 2; base = b; }
+    __device__ __forceinline__ void shadow(V3&, const Ray& r, float tmin, float tmax, bool test,
+                                           V3 c, int group_end) {
+        if (n >= A.maxS) {
+            atomicOr(A.status, 1);
+            return;
+        }
+        size_t k = (size_t)n * A.Q + slot;
+        A.sh_o[k] = make_float4(r.o.x, r.o.y, r.o.z, tmin);
+        A.sh_d[k] = make_float4(r.d.x, r.d.y, r.d.z, tmax);
+        A.sh_c[k] = make_float4(c.x, c.y, c.z, __int_as_float((test ? 1 : 0) | (group_end << 1)));
+        ++n;
+    }
+    __device__ __forceinline__ void pending(V3 tl, V3 ww, float ss) { tail = tl; w = ww; s = ss; }
+    __device__ __forceinline__ void store() {
+        A.pb[slot] = make_float4(base.x, base.y, base.z, __int_as_float(n));
+        A.pt[slot] = make_float4(tail.x, tail.y, tail.z, s);
+        A.pw[slot] = make_float4(w.x, w.y, w.z, __int_as_float(kind));
+    }
+};
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kWfBlock)
+wf_shade(WfArgs A, int it) {
+    RayCount rc = {};
+    QView qv = qview(A, it);
+    unsigned int* cursor = A.work + it * 3 + 1;
+    int* qout = A.q[(it + 1) & 1];
+    int* cout = A.counts + (it + 1) * kOctants;
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        int base = fetch32(cursor);
+        if (base >= qv.total) break;
+        int e = base + lane;
+        bool alive = false;
+        int slot = -1;
+        int bin = 0;
+        if (e < qv.total) {
+            slot = qv.slot(e);
+            uint4 stv = A.st[slot];
+            const WfJob& J = A.jobs[stv.w];
+            const SceneView& S = A.views[J.view];
+            float4 o = A.ray_o[slot], d = A.ray_d[slot], T = A.T[slot], L = A.L[slot];
+            float4 hv = A.hit[slot];
+            PathState ps;
+            ps.ray = Ray{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)};
+            ps.T = v3(T.x, T.y, T.z);
+            ps.L = v3(L.x, L.y, L.z);
+            ps.rng.s = stv.x;
+            ps.depth = (int)stv.y;
+            ps.flags = stv.z;
+            int leaf = __float_as_int(hv.z);
+            Hit h;
+            bool found = leaf >= 0;
+            if (found) make_hit(S, __float_as_int(hv.y), leaf, ps.ray, 1e-4f, hv.x, h);
+            StoreNee E(A, slot);
+            alive = shade_vertex(S, J.P, ps, found, h, E);
+            E.store();
+            if (COUNT) {
+                rc.shadow += E.n;
+                if (alive && (ps.flags & kFlagWhitted)) rc.ref++;
+            }
+            A.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 0.0f);
+            if (alive) {
+                A.ray_o[slot] = make_float4(ps.ray.o.x, ps.ray.o.y, ps.ray.o.z, 0.0f);
+                A.ray_d[slot] = make_float4(ps.ray.d.x, ps.ray.d.y, ps.ray.d.z, 0.0f);
+                A.T[slot] = make_float4(ps.T.x, ps.T.y, ps.T.z, 0.0f);
+                A.st[slot] = make_uint4(ps.rng.s, (unsigned)ps.depth, ps.flags, stv.w);
+                if (A.sort_key == 1)
+                    bin = (ps.ray.d.x < 0.0f ? 1 : 0) | (ps.ray.d.y < 0.0f ? 2 : 0) |
+                          (ps.ray.d.z < 0.0f ? 4 : 0);
+            }
+        }
+        // warp-aggregated append, one atomic per (warp, bin)
+        const int nbins = A.sort_key == 1 ? kOctants : 1;
+#pragma unroll 1
+        for (int b = 0; b < nbins; ++b) {
+            unsigned m = __ballot_sync(0xffffffffu, alive && bin == b);
+            if (!m) continue;
+            int first = 0;
+            if (lane == __ffs(m) - 1) first = atomicAdd(cout + b, __popc(m));
+            first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
+            if (alive && bin == b) qout[b * A.Q + first + __popc(m & ((1u << lane) - 1u))] = slot;
+        }
+    }
+    flush_counts<COUNT>(A, rc);
+}
+
+// ---- shadow -------------------------------------------------------------------
+template <bool COUNT>
+__global__ void __launch_bounds__(kWfBlock)
+wf_shadow(WfArgs A, int it) {
+    extern __shared__ int smem[];
+    TravStack<kWfShared> stk;
+    stk.sref = smem + threadIdx.x;
+    stk.st = reinterpret_cast<float*>(smem + kWfShared * blockDim.x) + threadIdx.x;
+    stk.stride = blockDim.x;
+    RayCount rc = {};
+    QView qv = qview(A, it);
+    unsigned int* cursor = A.work + it * 3 + 2;
+    while (true) {
+        int base = fetch32(cursor);
+        if (base >= qv.total) break;
+        int e = base + (threadIdx.x & 31);
+        if (e < qv.total) {
+            int slot = qv.slot(e);
+            float4 pw = A.pw[slot];
+            int kind = __float_as_int(pw.w);
+            if (kind != 0) {
+                float4 pb = A.pb[slot], pt = A.pt[slot], L4 = A.L[slot];
+                const SceneView& S = A.views[A.jobs[A.st[slot].w].view];
+                NeeAccum acc;
+                if (kind == 1) acc.begin_pt();
+                else acc.begin_whitted(v3(pb.x, pb.y, pb.z));
+                V3 L = v3(L4.x, L4.y, L4.z);
+                int n = __float_as_int(pb.w);
+                for (int k = 0; k < n; ++k) {
+                    size_t idx = (size_t)k * A.Q + slot;
+                    float4 so = A.sh_o[idx], sd = A.sh_d[idx], sc = A.sh_c[idx];
+                    int bits = __float_as_int(sc.w);
+                    bool vis = true;
+                    if (bits & 1) {
+                        Ray r{v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z)};
+                        vis = !any_hit<kWfShared, COUNT>(S, r, so.w, sd.w, stk, &rc.tc);
+                    }
+                    acc.add(L, v3(sc.x, sc.y, sc.z), bits >> 1, vis);
+                }
+                acc.finish(L, v3(pt.x, pt.y, pt.z), v3(pw.x, pw.y, pw.z), pt.w);
+                A.L[slot] = make_float4(L.x, L.y, L.z, 0.0f);
+            }
+        }
+    }
+    flush_counts<COUNT>(A, rc);
+}
+
+// ---- accumulate -----------------------------------------------------------------
+// One thread per pixel of the chunk: sums in the megakernel's lane order
+// (lane g takes samples g, g+G, ...; lanes combined by a butterfly).
+__global__ void __launch_bounds__(kWfBlock)
+wf_accumulate(WfArgs A, long long pix_begin, int n_pix, long long path_begin) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_pix) return;
+    long long pix = pix_begin + k;
+    int jb = find_job_pix(A.jobs, A.n_jobs, pix);
+    const WfJob& J = A.jobs[jb];
+    int spp = J.P.spp, G = J.G;
+    long long lp = pix - J.pix_off;
+    long long first = J.path_off + lp * spp - path_begin;
+    V3 acc[32], acc2[32];
+    for (int g = 0; g < G; ++g) { acc[g] = v3(0, 0, 0); acc2[g] = v3(0, 0, 0); }
+    for (int g = 0; g < G; ++g) {
+        for (int s = g; s < spp; s += G) {
+            float4 l = A.L[first + s];
+            V3 c = v3(l.x, l.y, l.z);
+            acc[g] = acc[g] + c;
+            acc2[g] = acc2[g] + c * c;
+        }
+    }
+    for (int off = G >> 1; off > 0; off >>= 1) {
+        for (int g = 0; g < off; ++g) {
+            acc[g] = acc[g] + acc[g + off];
+            acc2[g] = acc2[g] + acc2[g + off];
+        }
+    }
+    const float denom = (float)spp;
+    float* o = J.out + 3 * lp;
+    o[0] = acc[0].x / denom;
+    o[1] = acc[0].y / denom;
+    o[2] = acc[0].z / denom;
+    if (J.m2) {
+        float* q = J.m2 + 3 * lp;
+        q[0] = acc2[0].x / denom;
+        q[1] = acc2[0].y / denom;
+        q[2] = acc2[0].z / denom;
+    }
+}
+
+// ---- host side ------------------------------------------------------------------
+struct WfPlanJob {
+    const SceneView* view;
+    RenderCfg cfg;
+    float* out;
+    float* m2;
+};
+
+static int lanes_for(int spp) {
+    int lim = spp < 32 ? spp : 32, G = 1;
+    while (G * 2 <= lim) G *= 2;
+    return G;
+}
+
+// Scratch of the wavefront, owned by the context (grown on demand).
+struct WfScratch {
+    void* mem = nullptr;
+    size_t bytes = 0;
+    int Q = 0;
+    int maxS = 0;
+    int iters = 0;
+    int jobs_cap = 0;
+    int views_cap = 0;
+    WfArgs args{};
+    SceneView* d_views = nullptr;
+    WfJob* d_jobs = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    unsigned long long graph_key = 0;
+};
+
+static size_t al(size_t x) { return (x + 255) & ~size_t(255); }
+
+static cudaError_t ensure_scratch(WfScratch& W, int Q, int maxS, int iters, int n_jobs,
+                                  int n_views) {
+    if (W.mem && W.Q >= Q && W.maxS >= maxS && W.iters >= iters && W.jobs_cap >= n_jobs &&
+        W.views_cap >= n_views)
+        return cudaSuccess;
+    if (W.graph) { cudaGraphExecDestroy(W.graph); W.graph = nullptr; W.graph_key = 0; }
+    if (W.mem) cudaFree(W.mem);
+    W.mem = nullptr;
+    Q = std::max(Q, W.Q);
+    maxS = std::max(std::max(maxS, W.maxS), 1);
+    iters = std::max(iters, W.iters);
+    n_jobs = std::max(n_jobs, W.jobs_cap);
+    n_views = std::max(n_views, W.views_cap);
+    size_t per = al((size_t)Q * 16);
+    size_t sz = 0;
+    sz += 9 * per;                                   // ray_o ray_d T L st hit pb pt pw
+    sz += 3 * (size_t)maxS * per;                    // shadow records
+    sz += 2 * al((size_t)kOctants * Q * 4);          // queues
+    sz += al((size_t)(iters + 2) * kOctants * 4);    // counts
+    sz += al((size_t)(iters + 2) * 3 * 4);           // work cursors
+    sz += al(4);                                     // status
+    sz += al((size_t)n_views * sizeof(SceneView));
+    sz += al((size_t)n_jobs * sizeof(WfJob));
+    cudaError_t e = cudaMalloc(&W.mem, sz);
+    if (e != cudaSuccess) { W.mem = nullptr; W.bytes = 0; W.Q = 0; return e; }
+    W.bytes = sz;
+    W.Q = Q;
+    W.maxS = maxS;
+    W.iters = iters;
+    W.jobs_cap = n_jobs;
+    W.views_cap = n_views;
+    unsigned char* p = static_cast<unsigned char*>(W.mem);
+    auto take = [&](size_t b) { unsigned char* r = p; p += al(b); return r; };
+    WfArgs& A = W.args;
+    A.Q = Q;
+    A.maxS = maxS;
+    A.ray_o = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.ray_d = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.T = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.L = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.st = reinterpret_cast<uint4*>(take((size_t)Q * 16));
+    A.hit = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.pb = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.pt = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.pw = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.sh_o = reinterpret_cast<float4*>(take((size_t)maxS * Q * 16));
+    A.sh_d = reinterpret_cast<float4*>(take((size_t)maxS * Q * 16));
+    A.sh_c = reinterpret_cast<float4*>(take((size_t)maxS * Q * 16));
+    A.q[0] = reinterpret_cast<int*>(take((size_t)kOctants * Q * 4));
+    A.q[1] = reinterpret_cast<int*>(take((size_t)kOctants * Q * 4));
+    A.counts = reinterpret_cast<int*>(take((size_t)(iters + 2) * kOctants * 4));
+    A.work = reinterpret_cast<unsigned int*>(take((size_t)(iters + 2) * 3 * 4));
+    A.status = reinterpret_cast<int*>(take(4));
+    W.d_views = reinterpret_cast<SceneView*>(take((size_t)n_views * sizeof(SceneView)));
+    W.d_jobs = reinterpret_cast<WfJob*>(take((size_t)n_jobs * sizeof(WfJob)));
+    A.views = W.d_views;
+    A.jobs = W.d_jobs;
+    return cudaSuccess;
+}
+
+// Shadow records a vertex can make: path-trace (point/directional lights +
+// quad lights) or Whitted (soft samples of every point/directional light).
+static int max_shadow_records(const SceneView& v, const std::vector<DevLight>& lights, int soft) {
+    int pt = 0, wh = 0;
+    for (const auto& l : lights) {
+        pt += 1;
+        if (l.kind != 2) wh += l.radius > 0.0f ? soft : 1;
+    }
+    (void)v;
+    return std::max(1, std::max(pt, wh));
+}
+
+struct WfOccupancy {
+    int grid_extend = 0, grid_shade = 0, grid_shadow = 0;
+};
+
+template <bool COUNT>
+static cudaError_t occupancy(WfOccupancy& o) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t smem = (size_t)kWfShared * kWfBlock * 8;
+    int b1 = 0, b2 = 0, b3 = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, wf_extend<COUNT>, kWfBlock, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, wf_shade<COUNT>, kWfBlock, 0);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, wf_shadow<COUNT>, kWfBlock, smem);
+    o.grid_extend = sms * std::max(b1, 1);
+    o.grid_shade = sms * std::max(b2, 1);
+    o.grid_shadow = sms * std::max(b3, 1);
+    return e;
+}
+
+// Enqueue the kernels of the whole path space on `st` (captured into a graph
+// by the caller).
+template <bool COUNT>
+static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& jobs, int iters,
+                                 int Qeff, cudaStream_t st, int* launches) {
+    WfOccupancy occ;
+    cudaError_t e = occupancy<COUNT>(occ);
+    if (e != cudaSuccess) return e;
+    const WfArgs& A = W.args;
+    const size_t smem = (size_t)kWfShared * kWfBlock * 8;
+    // walk the path space in chunks of whole pixels
+    int ji = 0;
+    long long pix_in_job = 0;
+    const int n_jobs = (int)jobs.size();
+    int n_launch = 0;
+    while (ji < n_jobs) {
+        long long path_begin = jobs[ji].path_off + pix_in_job * jobs[ji].P.spp;
+        long long pix_begin = jobs[ji].pix_off + pix_in_job;
+        long long slots = 0, pixels = 0;
+        while (ji < n_jobs) {
+            const WfJob& J = jobs[ji];
+            long long npix = (long long)J.P.W * J.P.H;
+            long long room = (Qeff - slots) / J.P.spp;
+            long long take = std::min(room, npix - pix_in_job);
+            if (take <= 0) break;
+            slots += take * J.P.spp;
+            pixels += take;
+            pix_in_job += take;
+            if (pix_in_job == npix) { ++ji; pix_in_job = 0; }
+        }
+        if (slots == 0) return cudaErrorInvalidValue;   // a pixel larger than Q
+        size_t cnt_bytes = (size_t)(iters + 2) * kOctants * 4;
+        if ((e = cudaMemsetAsync(A.counts, 0, cnt_bytes, st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(A.work, 0, (size_t)(iters + 2) * 3 * 4, st)) != cudaSuccess) return e;
+        int gblocks = (int)((slots + kWfBlock - 1) / kWfBlock);
+        wf_generate<COUNT><<<gblocks, kWfBlock, 0, st>>>(A, path_begin, (int)slots);
+        n_launch += 1;
+        for (int it = 0; it < iters; ++it) {
+            wf_extend<COUNT><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
+            wf_shade<COUNT><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
+            wf_shadow<COUNT><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
+            n_launch += 3;
+        }
+        int ablocks = (int)((pixels + kWfBlock - 1) / kWfBlock);
+        wf_accumulate<<<ablocks, kWfBlock, 0, st>>>(A, pix_begin, (int)pixels, path_begin);
+        n_launch += 1;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (launches) *launches = n_launch;
+    return cudaSuccess;
+}
+
+// Render jobs through the wavefront. Views/lights are host copies used to
+// size the scratch; `views_dev_src` are the SceneViews to upload.
+cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
+                             const std::vector<std::vector<DevLight>>& lights,
+                             const std::vector<int>& job_view, const std::vector<RenderCfg>& cfgs,
+                             const std::vector<float*>& outs, const std::vector<float*>& m2s,
+                             unsigned long long* counters, cudaStream_t st, bool use_graph,
+                             int* launches, int* status_out) {
+    const int n = (int)cfgs.size();
+    std::vector<WfJob> jobs(n);
+    long long path_off = 0, pix_off = 0;
+    int iters = 0, maxS = 1, max_spp = 1;
+    long long total_paths = 0;
+    bool count = false;
+    int qcap = 0, sort_key = 0;
+    for (int k = 0; k < n; ++k) {
+        const RenderCfg& c = cfgs[k];
+        WfJob& J = jobs[k];
+        J.P = PathParams{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias,
+                         c.salt, c.sample_offset};
+        J.view = job_view[k];
+        J.path_off = path_off;
+        J.pix_off = pix_off;
+        J.G = lanes_for(c.spp);
+        J.out = outs[k];
+        J.m2 = m2s[k];
+        path_off += (long long)c.W * c.H * c.spp;
+        pix_off += (long long)c.W * c.H;
+        iters = std::max(iters, c.depth);
+        max_spp = std::max(max_spp, c.spp);
+        maxS = std::max(maxS, max_shadow_records(views[J.view], lights[J.view], c.soft));
+        count = count || c.count;
+        if (c.queue_capacity > 0) qcap = c.queue_capacity;
+        sort_key = c.sort_key;
+    }
+    total_paths = path_off;
+    long long Q = qcap > 0 ? qcap : (1LL << 21);
+    Q = std::max<long long>(Q, max_spp);
+    Q = std::min<long long>(Q, total_paths);
+    Q = std::max<long long>(Q, 1);
+    cudaError_t e = ensure_scratch(W, (int)Q, maxS, iters, n, (int)views.size());
+    if (e != cudaSuccess) return e;
+    W.args.n_jobs = n;
+    W.args.counters = counters;
+    W.args.sort_key = sort_key;
+    W.args.maxS = maxS;
+    if ((e = cudaMemcpyAsync(W.d_views, views.data(), views.size() * sizeof(SceneView),
+                             cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(W.d_jobs, jobs.data(), jobs.size() * sizeof(WfJob),
+                             cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemsetAsync(W.args.status, 0, 4, st)) != cudaSuccess) return e;
+    // A graph is reused while the frame's shape is unchanged.
+    unsigned long long key = 1469598103934665603ull;
+    auto mix = [&](unsigned long long v) { key = (key ^ v) * 1099511628211ull; };
+    mix((unsigned long long)n);
+    mix((unsigned long long)Q);
+    mix((unsigned long long)maxS);
+    mix((unsigned long long)sort_key);
+    mix((unsigned long long)count);
+    for (const auto& J : jobs) {
+        mix((unsigned long long)J.P.W); mix((unsigned long long)J.P.H);
+        mix((unsigned long long)J.P.spp); mix((unsigned long long)J.P.depth);
+    }
+    mix((unsigned long long)iters);
+    int nl = 0;
+    if (use_graph) {
+        if (!W.graph || W.graph_key != key) {
+            if (W.graph) { cudaGraphExecDestroy(W.graph); W.graph = nullptr; }
+            cudaGraph_t g = nullptr;
+            if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+                return e;
+            cudaError_t ee = count ? enqueue_frame<true>(W, jobs, iters, (int)Q, st, &nl)
+                                   : enqueue_frame<false>(W, jobs, iters, (int)Q, st, &nl);
+            e = cudaStreamEndCapture(st, &g);
+            if (ee != cudaSuccess) { if (g) cudaGraphDestroy(g); return ee; }
+            if (e != cudaSuccess) return e;
+            e = cudaGraphInstantiate(&W.graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) { W.graph = nullptr; return e; }
+            W.graph_key = key;
+        }
+        if ((e = cudaGraphLaunch(W.graph, st)) != cudaSuccess) return e;
+        if (launches) *launches = 1;
+    } else {
+        e = count ? enqueue_frame<true>(W, jobs, iters, (int)Q, st, &nl)
+                  : enqueue_frame<false>(W, jobs, iters, (int)Q, st, &nl);
+        if (e != cudaSuccess) return e;
+        if (launches) *launches = nl;
+    }
+    if (status_out) {
+        if ((e = cudaMemcpyAsync(status_out, W.args.status, 4, cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
+void wavefront_release(WfScratch& W) {
+    if (W.graph) cudaGraphExecDestroy(W.graph);
+    W.graph = nullptr;
+    if (W.mem) cudaFree(W.mem);
+    W.mem = nullptr;
+    W.bytes = 0;
+    W.Q = 0;
+}
+
+WfScratch* wavefront_new() { return new WfScratch(); }
+void wavefront_delete(WfScratch* W) {
+    if (!W) return;
+    wavefront_release(*W);
+    delete W;
+}
+
+}  // namespace pgpu
