@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Benchmark of the GPU path-tracing core.
+
+Workload (the sphere-cloud configuration): 100,000 seeded random spheres
+(60/30/10 diffuse/metal/glass), one directional light, sky 0.3; 1280x720,
+n=4 (16 spp), depth 8; 14,745,600 paths per frame. A step renders one frame.
+
+  value   Mpaths/s of the wavefront engine with the scene resident in HBM and
+          the image written to device memory (CUDA events on the render
+          stream, L2 flushed between steps outside the timed events)
+  e2e     the same metric through the C-ABI as Pencil's --gpu mode calls it:
+          every step uploads the scene from pinned host memory
+          (pgpu_upload_scene), renders into a pinned host image (pgpu_render)
+          and frees the scene
+  extras  the megakernel's Mpaths/s on the same frame (the images are
+          bit-identical, so equal RMSE), Mrays/s, per-kernel roofline
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank renders the frame with its own sample
+offset (weak scaling: per-GPU work fixed) and the HDR images are summed with
+one NCCL all-reduce per step, inside the timed region. `--impl reference`
+times the reference CPU renderer (oracle/_ref, built from the reference's
+own sources; the C oracle port where it is absent) on a bounded sample of
+the same workload on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = ("Mpaths/s & Mrays/s at equal RMSE, wavefront vs megakernel (1 B200); "
+          "adjoint ms/grad")
+WORKLOAD = "sphere_cloud_100k_1280x720_n4_16spp_depth8"
+CPU_SAMPLE = (320, 180, 4, 8)      # width, height, n, depth of the bounded CPU sample
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-case", choices=["wavefront", "megakernel"], default=None,
+                    help="render the workload once, kernels launched one by one (for ncu)")
+    ap.add_argument("--profile-scale", type=int, default=1,
+                    help="divide the image width and height by this (smaller ncu cases)")
+    return ap.parse_args()
+
+
+# ---- clocks ---------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples (every 200 ms) while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.out.flush()
+        rows = []
+        for line in Path(self.out.name).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---- CPU reference ----------------------------------------------------------------
+def cpu_reference_run(scene, steps: int, warmup: int) -> dict:
+    """Time the reference CPU renderer on the bounded sample: seconds per run."""
+    from oracle import oracle as O
+    w, h, n, depth = CPU_SAMPLE
+    threads = os.cpu_count() or 1
+    paths = w * h * n * n
+    if O.ref_available():
+        _, info = O.ref_render(scene, w, h, n, depth, True, threads=threads,
+                               repeat=warmup + steps, want_image=False)
+        secs = info["seconds"][warmup:]
+        kind = "reference"
+    else:
+        from pencil_b200.renderer import RenderSettings
+        orc = O.Oracle(scene)
+        st = RenderSettings(width=w, height=h, samples=n, pathtrace=True, pathtrace_bounces=depth)
+        secs = []
+        for k in range(warmup + steps):
+            t = time.perf_counter()
+            orc.render(st, threads=threads)
+            if k >= warmup:
+                secs.append(time.perf_counter() - t)
+        kind = "port"
+    med = statistics.median(secs)
+    return {"value": paths / med / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": kind,
+            "sample": f"the same 100k-sphere scene at {w}x{h}, n={n} ({n*n} spp), depth {depth}: "
+                      f"{paths} paths per run, median of {len(secs)} runs",
+            "seconds": secs}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from pencil_b200 import workloads as W
+    wl = W.sphere_cloud()
+    steps, warmup = max(args.steps, 1), max(args.warmup, 0)
+    # each step is one bounded-sample render; keep the whole run to a few minutes
+    steps = min(steps, 10)
+    warmup = min(warmup, 3)
+    cb = cpu_reference_run(wl.scene, steps, warmup)
+    ms = statistics.median(cb["seconds"]) * 1e3
+    line = {"metric": METRIC, "value": cb["value"], "unit": "Mpaths/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample": cb["sample"], "threads": cb["cores"]},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---- GPU ----------------------------------------------------------------------------
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def ncu_traffic_per_ray() -> float | None:
+    """DRAM bytes per extension ray of wf_extend, from the committed ncu
+    summary (profiles/wf_extend_sphere_cloud.txt), if present."""
+    p = ROOT / "profiles" / "wf_extend_sphere_cloud.txt"
+    if not p.exists():
+        return None
+    m = re.search(r"dram_bytes_per_ray:\s*([0-9.eE+-]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+def scene_bytes(scene) -> int:
+    """Bytes pgpu_upload_scene copies to the device: child-pair nodes, leaf
+    geometry (two float4), material and primitive ids, vertices, materials,
+    lights."""
+    n = scene.n_unified
+    n_tri = int((scene.prims["type"] == 1).sum()) + len(scene.mesh_indices)
+    verts = len(scene.mesh_vertices) + 3 * int((scene.prims["type"] == 1).sum())
+    return (max(n - 1, 0) * 64 + n * (16 + 16 + 4 + 4) + verts * 16 +
+            scene.n_materials * 64 + len(scene.lights) * 64) if n_tri >= 0 else 0
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+    from pencil_b200 import _abi as A
+    from pencil_b200 import workloads as W
+    from pencil_b200.renderer import GpuContext, RenderSettings, RenderStats
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    wl = W.sphere_cloud()
+    st: RenderSettings = wl.settings
+    st.sample_offset = rank * st.samples * st.samples
+    paths_per_frame = st.width * st.height * st.samples ** 2
+    ctx = GpuContext(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    sid = ctx.upload(wl.scene)
+    img = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(engine: int, steps: int, warmup: int, clocks=None):
+        st.engine = engine
+        for _ in range(warmup):
+            ctx.render_device(sid, st, img.data_ptr())
+            if world > 1:
+                with torch.cuda.stream(stream):
+                    dist.all_reduce(img)
+        evs = []
+        barrier()
+        cm = clocks if clocks is not None else _Null()
+        with cm:
+            for _ in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.render_device(sid, st, img.data_ptr())
+                if world > 1:
+                    with torch.cuda.stream(stream):
+                        dist.all_reduce(img)
+                e1.record(stream)
+                evs.append((e0, e1))
+            barrier()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        t = torch.tensor([ms], device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()) / steps
+
+    clocks = ClockSampler(local)
+    ms_wf = timed(A.ENGINE_WAVEFRONT, args.steps, args.warmup, clocks)
+    clk = clocks.summary()
+    mk_steps = max(2, min(args.steps, 5))
+    ms_mk = timed(A.ENGINE_MEGAKERNEL, mk_steps, 1)
+    value = paths_per_frame * world / (ms_wf * 1e-3) / 1e6
+    mk_value = paths_per_frame * world / (ms_mk * 1e-3) / 1e6
+
+    # instrumented runs (outside the timed region): ray/node counts, kernel times
+    st.engine = A.ENGINE_WAVEFRONT
+    cnt = RenderStats()
+    st.count_rays, st.count_nodes = True, True
+    ctx.render(sid, st, stats=cnt)
+    st.count_rays, st.count_nodes = False, False
+    prof = RenderStats()
+    st.profile_kernels = True
+    ctx.render(sid, st, stats=prof)
+    ctx.render(sid, st, stats=prof)
+    st.profile_kernels = False
+    rays = cnt.extension_rays + cnt.shadow_rays
+    mrays = rays * world / (ms_wf * 1e-3) / 1e6
+
+    # roofline of the dominant kernel (closest-hit traversal, wf_extend)
+    kms = prof.kernel_ms
+    dominant = max(("extend", "shade", "shadow", "generate", "accumulate"), key=lambda k: kms[k])
+    ext_launches = prof.kernel_launches and (prof.kernel_launches // max(1, 2 + 3 * st.pathtrace_bounces)) * st.pathtrace_bounces
+    per_ray_queue = 16 + 16 + 16 + 4 + 16            # ray o, d, state, queue slot; hit write
+    alg_bytes = cnt.ext_node_visits * 64 + cnt.ext_leaf_bytes + cnt.extension_rays * per_ray_queue
+    n_ext_launches = max(1, ext_launches)
+    achieved = alg_bytes / (kms["extend"] * 1e-3) / 1e9
+    peaks = measured_peaks()
+    tr = ncu_traffic_per_ray()
+    roof = {"kernel": "wf_extend", "bound": "hbm", "achieved": achieved,
+            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+            "traffic": (tr * cnt.extension_rays / n_ext_launches) if tr else None,
+            "algorithmic_bytes_per_launch": alg_bytes / n_ext_launches,
+            "launches": n_ext_launches,
+            "avg_launch_ms": kms["extend"] / n_ext_launches,
+            "peak_source": peaks["source"],
+            "bytes_per_ray": alg_bytes / max(1, cnt.extension_rays),
+            "nodes_per_ray": cnt.ext_node_visits / max(1, cnt.extension_rays),
+            "dominant_kernel_by_time": dominant,
+            "kernel_ms": kms}
+
+    # e2e through the C-ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_img = torch.empty((st.height, st.width, 3), dtype=torch.float32).pin_memory()
+        out_np = host_img.numpy()
+        h2d = scene_bytes(wl.scene)
+        d2h = out_np.nbytes
+        ctx.render(sid, st, out=out_np)
+        times = []
+        for k in range(args.warmup + args.steps):
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            s2 = ctx.upload(wl.scene)
+            ctx.render(s2, st, out=out_np)
+            ctx.free(s2)
+            dt = time.perf_counter() - t0
+            if k >= args.warmup:
+                times.append(dt)
+        sec = float(np.mean(times))
+        t = torch.tensor([sec], device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+        e2e = {"value": paths_per_frame * world / sec / 1e6, "unit": "Mpaths/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": sec * 1e3}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_reference_run(wl.scene, 1, 0)
+            cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unit": "Mpaths/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {ex}"}
+
+    launches_per_frame = prof.kernel_launches
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_wf,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded numpy scene; no dataset)",
+            "config": {"workload": WORKLOAD, "engine": "wavefront", "spheres": 100000,
+                       "width": st.width, "height": st.height, "spp": st.samples ** 2,
+                       "depth": st.pathtrace_bounces, "paths_per_step": paths_per_frame * world,
+                       "l2": "256 MiB memset between steps, outside the timed events",
+                       "parallelism": f"weak: {world} GPU(s), distinct sample offsets, "
+                                      "NCCL all-reduce of the image per step" if world > 1
+                                      else "1 GPU"},
+            "mrays_per_s": mrays,
+            "rays_per_step": rays,
+            "megakernel": {"value": mk_value, "unit": "Mpaths/s", "ms_per_step": ms_mk},
+            "wavefront_over_megakernel": ms_mk / ms_wf,
+            "equal_rmse": "bit-identical images (same estimator, same random numbers)",
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk,
+            "gpu_launches": launches_per_frame * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.free(sid)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def run_profile_case(args) -> None:
+    """One frame of the workload with no CUDA graph, for ncu captures."""
+    from pencil_b200 import _abi as A
+    from pencil_b200 import workloads as W
+    from pencil_b200.renderer import GpuContext, RenderStats
+    wl = W.sphere_cloud()
+    st = wl.settings
+    st.width //= args.profile_scale
+    st.height //= args.profile_scale
+    st.use_graph = False
+    st.engine = A.ENGINE_WAVEFRONT if args.profile_case == "wavefront" else A.ENGINE_MEGAKERNEL
+    ctx = GpuContext(0)
+    sid = ctx.upload(wl.scene)
+    stats = RenderStats()
+    img = ctx.render(sid, st, stats=stats)
+    assert np.isfinite(img).all()
+    print(json.dumps({"profile_case": args.profile_case, "width": st.width, "height": st.height,
+                      "launches": stats.kernel_launches, "device_ms": stats.device_ms}))
+    ctx.free(sid)
+    ctx.close()
+
+
+def main():
+    args = parse_args()
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

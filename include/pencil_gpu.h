@@ -205,8 +205,10 @@ enum pgpu_flags {
     PGPU_FLAG_DEVICE_OUTPUT = 1,  /* out_rgb / out_m2 are device pointers   */
     PGPU_FLAG_COUNT_RAYS    = 2,  /* fill the ray counters in pgpu_stats    */
     PGPU_FLAG_COUNT_NODES   = 4,  /* also count node visits / prim tests    */
-    PGPU_FLAG_NO_GRAPH      = 8   /* wavefront: launch kernels one by one
+    PGPU_FLAG_NO_GRAPH      = 8,  /* wavefront: launch kernels one by one
                                      instead of replaying a CUDA graph       */
+    PGPU_FLAG_PROFILE_KERNELS = 16 /* time each kernel class (implies
+                                     NO_GRAPH); see pgpu_stats.kernel_ms     */
 };
 
 typedef struct pgpu_render_params {
@@ -236,8 +238,16 @@ typedef struct pgpu_stats {
                                   (src/renderer.hpp:404, 830)               */
     uint64_t node_visits;      /* interior nodes fetched (COUNT_NODES)       */
     uint64_t prim_tests;       /* primitive tests (COUNT_NODES)              */
+    uint64_t ext_node_visits;  /* of which by closest-hit traversal          */
+    uint64_t ext_leaf_bytes;   /* leaf bytes read by closest-hit traversal   */
+    uint64_t shadow_node_visits; /* of which by any-hit traversal            */
+    uint64_t shadow_leaf_bytes;  /* leaf bytes read by any-hit traversal     */
     double   device_ms;        /* device time of the render kernels          */
     double   total_ms;         /* wall time of the call                      */
+    /* PGPU_FLAG_PROFILE_KERNELS: device time per kernel class (generate,
+     * extend, shade, shadow, accumulate, megakernel), from CUDA events
+     * around every launch (kernels are then launched one by one). */
+    double   kernel_ms[6];
     int32_t  kernel_launches;  /* kernels launched by the call               */
     int32_t  reserved;
 } pgpu_stats;

@@ -34,6 +34,8 @@ ENGINE_WAVEFRONT, ENGINE_MEGAKERNEL = 0, 1
 RNG_COUNTER, RNG_PIXEL_SEQUENTIAL = 0, 1
 GLASS_FRESNEL_SPLIT, GLASS_BOTH_BRANCHES = 0, 1
 FLAG_DEVICE_OUTPUT, FLAG_COUNT_RAYS, FLAG_COUNT_NODES, FLAG_NO_GRAPH = 1, 2, 4, 8
+FLAG_PROFILE_KERNELS = 16
+KERNEL_CLASSES = ("generate", "extend", "shade", "shadow", "accumulate", "megakernel")
 
 PRIM_DTYPE = np.dtype([("type", "<i4"), ("material", "<i4"), ("p", "<f4", (14,))])
 NODE_DTYPE = np.dtype([("bmin", "<f4", (3,)), ("left", "<i4"), ("bmax", "<f4", (3,)),
@@ -81,11 +83,16 @@ class Stats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("extension_rays", C.c_uint64),
                 ("shadow_rays", C.c_uint64), ("reference_rays", C.c_uint64),
                 ("node_visits", C.c_uint64), ("prim_tests", C.c_uint64),
+                ("ext_node_visits", C.c_uint64), ("ext_leaf_bytes", C.c_uint64),
+                ("shadow_node_visits", C.c_uint64), ("shadow_leaf_bytes", C.c_uint64),
                 ("device_ms", C.c_double), ("total_ms", C.c_double),
+                ("kernel_ms", C.c_double * 6),
                 ("kernel_launches", C.c_int32), ("reserved", C.c_int32)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "kernel_ms")}
+        d["kernel_ms"] = dict(zip(KERNEL_CLASSES, list(self.kernel_ms)))
+        return d
 
 
 EXPORTS = {

@@ -31,7 +31,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
                              const std::vector<int>& job_view, const std::vector<RenderCfg>& cfgs,
                              const std::vector<float*>& outs, const std::vector<float*>& m2s,
                              unsigned long long* counters, cudaStream_t st, bool use_graph,
-                             int* launches, int* status_out);
+                             int* launches, int* status_out, double* kernel_ms);
 
 constexpr int kMaxDepth = 64;          // traversal stack bound (kMaxStack)
 constexpr int kMaxTreeFrames = 32;     // Whitted recursion bound of the two-branch mode
@@ -111,6 +111,8 @@ struct pgpu_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     WfScratch* wf = nullptr;
     int* h_status = nullptr;          // pinned
+    unsigned char* h_stage = nullptr; // pinned staging of scene uploads
+    size_t stage_cap = 0;
 };
 
 namespace {
@@ -259,6 +261,7 @@ void pgpu_destroy(pgpu_ctx* c) {
     cudaFree(c->d_query);
     wavefront_delete(c->wf);
     if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own) cudaStreamDestroy(c->own);
@@ -410,13 +413,24 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     size_t off_mt = align256(off_lp + (size_t)n_leaf * 4);
     size_t off_lt = align256(off_mt + mats.size() * sizeof(DevMaterial));
     size_t total = align256(off_lt + lights.size() * sizeof(DevLight));
-    std::vector<unsigned char> host(total, 0);
-    float4* h_nodes = reinterpret_cast<float4*>(host.data() + off_nodes);
-    float4* h_ga = reinterpret_cast<float4*>(host.data() + off_ga);
-    float4* h_gb = reinterpret_cast<float4*>(host.data() + off_gb);
-    float4* h_vt = reinterpret_cast<float4*>(host.data() + off_vt);
-    int* h_lm = reinterpret_cast<int*>(host.data() + off_lm);
-    int* h_lp = reinterpret_cast<int*>(host.data() + off_lp);
+    if (c->stage_cap < total) {
+        if (c->h_stage) cudaFreeHost(c->h_stage);
+        c->h_stage = nullptr;
+        c->stage_cap = 0;
+        if (cudaMallocHost(reinterpret_cast<void**>(&c->h_stage), total) != cudaSuccess) {
+            c->h_stage = nullptr;
+            return fail(c, PGPU_ERR_OUT_OF_MEMORY, "pinned staging of %zu bytes", total);
+        }
+        c->stage_cap = total;
+    }
+    unsigned char* host = c->h_stage;
+    std::memset(host, 0, total);
+    float4* h_nodes = reinterpret_cast<float4*>(host + off_nodes);
+    float4* h_ga = reinterpret_cast<float4*>(host + off_ga);
+    float4* h_gb = reinterpret_cast<float4*>(host + off_gb);
+    float4* h_vt = reinterpret_cast<float4*>(host + off_vt);
+    int* h_lm = reinterpret_cast<int*>(host + off_lm);
+    int* h_lp = reinterpret_cast<int*>(host + off_lp);
     for (int k = 0; k < s->n_mesh_vertices; ++k)
         h_vt[k] = make_float4(s->mesh_vertices[3 * k], s->mesh_vertices[3 * k + 1],
                               s->mesh_vertices[3 * k + 2], 0.0f);
@@ -479,8 +493,8 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
                 break;
         }
     }
-    std::memcpy(host.data() + off_mt, mats.data(), mats.size() * sizeof(DevMaterial));
-    std::memcpy(host.data() + off_lt, lights.data(), lights.size() * sizeof(DevLight));
+    std::memcpy(host + off_mt, mats.data(), mats.size() * sizeof(DevMaterial));
+    std::memcpy(host + off_lt, lights.data(), lights.size() * sizeof(DevLight));
 
     PGPU_CUDA(c, cudaSetDevice(c->device));
     auto ds = std::make_unique<DeviceScene>();
@@ -489,7 +503,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         return fail(c, PGPU_ERR_OUT_OF_MEMORY, "scene arena of %zu bytes: %s", total,
                     cudaGetErrorString(e));
     ds->bytes = total;
-    e = cudaMemcpyAsync(ds->arena, host.data(), total, cudaMemcpyHostToDevice, c->stream);
+    e = cudaMemcpyAsync(ds->arena, host, total, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
         cudaFree(ds->arena);
@@ -614,6 +628,7 @@ int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, Re
     cfg.block = p->block_size;
     cfg.queue_capacity = p->queue_capacity;
     cfg.sort_key = p->sort_key;
+    cfg.profile = (p->flags & PGPU_FLAG_PROFILE_KERNELS) != 0;
     (void)ds;
     return PGPU_OK;
 }
@@ -621,7 +636,8 @@ int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, Re
 // Run jobs through the wavefront engine; checks the device status word.
 int run_wavefront(pgpu_ctx* c, const std::vector<DeviceScene*>& scenes,
                   const std::vector<RenderCfg>& cfgs, const std::vector<float*>& outs,
-                  const std::vector<float*>& m2s, bool use_graph, int* launches) {
+                  const std::vector<float*>& m2s, bool use_graph, int* launches,
+                  double* kernel_ms) {
     std::vector<SceneView> views;
     std::vector<std::vector<DevLight>> lights;
     std::vector<int> job_view;
@@ -640,7 +656,7 @@ int run_wavefront(pgpu_ctx* c, const std::vector<DeviceScene*>& scenes,
     }
     *c->h_status = 0;
     cudaError_t e = wavefront_render(*c->wf, views, lights, job_view, cfgs, outs, m2s, c->d_cnt,
-                                     c->stream, use_graph, launches, c->h_status);
+                                     c->stream, use_graph, launches, c->h_status, kernel_ms);
     if (e != cudaSuccess) return cuda_fail(c, e, "wavefront launch");
     return PGPU_OK;
 }
@@ -675,6 +691,7 @@ int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float*
     if (cfg.count)
         PGPU_CUDA(c, cudaMemsetAsync(c->d_cnt, 0, CNT_N * sizeof(unsigned long long), c->stream));
     int launches = 1;
+    double kms[KC_N] = {0};
     PGPU_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     cudaError_t e;
     if (cfg.engine == PGPU_ENGINE_MEGAKERNEL) {
@@ -683,7 +700,7 @@ int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float*
     } else {
         *c->h_status = 0;
         rc = run_wavefront(c, {ds}, {cfg}, {d_out}, {d_m2}, (p->flags & PGPU_FLAG_NO_GRAPH) == 0,
-                           &launches);
+                           &launches, cfg.profile ? kms : nullptr);
         if (rc) return rc;
     }
     PGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
@@ -709,6 +726,12 @@ int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float*
         stats->reference_rays = cnt[CNT_REF];
         stats->node_visits = cnt[CNT_NODES];
         stats->prim_tests = cnt[CNT_PRIMS];
+        stats->ext_node_visits = cnt[CNT_NODES_EXT];
+        stats->ext_leaf_bytes = cnt[CNT_LEAF_EXT];
+        stats->shadow_node_visits = cnt[CNT_NODES_SH];
+        stats->shadow_leaf_bytes = cnt[CNT_LEAF_SH];
+        if (cfg.engine == PGPU_ENGINE_MEGAKERNEL && cfg.profile) kms[KC_MEGAKERNEL] = ms;
+        for (int k = 0; k < KC_N; ++k) stats->kernel_ms[k] = kms[k];
         stats->kernel_launches = launches;
         stats->total_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -756,8 +779,10 @@ int32_t pgpu_render_batch(pgpu_ctx* c, int32_t n_jobs, const int32_t* ids,
     if (count) PGPU_CUDA(c, cudaMemsetAsync(c->d_cnt, 0, CNT_N * sizeof(unsigned long long), c->stream));
     int launches = 0;
     PGPU_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    double kms[KC_N] = {0};
+    const bool prof = (params[0].flags & PGPU_FLAG_PROFILE_KERNELS) != 0;
     int rc = run_wavefront(c, scenes, cfgs, d_outs, d_m2s, (params[0].flags & PGPU_FLAG_NO_GRAPH) == 0,
-                           &launches);
+                           &launches, prof ? kms : nullptr);
     if (rc) return rc;
     PGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     if (!dev_out)
@@ -780,6 +805,11 @@ int32_t pgpu_render_batch(pgpu_ctx* c, int32_t n_jobs, const int32_t* ids,
         stats->reference_rays = cnt[CNT_REF];
         stats->node_visits = cnt[CNT_NODES];
         stats->prim_tests = cnt[CNT_PRIMS];
+        stats->ext_node_visits = cnt[CNT_NODES_EXT];
+        stats->ext_leaf_bytes = cnt[CNT_LEAF_EXT];
+        stats->shadow_node_visits = cnt[CNT_NODES_SH];
+        stats->shadow_leaf_bytes = cnt[CNT_LEAF_SH];
+        for (int k = 0; k < KC_N; ++k) stats->kernel_ms[k] = kms[k];
         stats->kernel_launches = launches;
         stats->total_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -27,6 +27,7 @@ struct RenderCfg {
     int block;
     int queue_capacity;
     int sort_key;
+    bool profile;
 };
 
 // Device counters written by the kernels (atomic adds).
@@ -37,7 +38,14 @@ enum DevCounter {
     CNT_NODES = 3,
     CNT_LEAF_BYTES = 4,
     CNT_PRIMS = 5,
-    CNT_N = 8
+    CNT_NODES_EXT = 6,
+    CNT_LEAF_EXT = 7,
+    CNT_NODES_SH = 8,
+    CNT_LEAF_SH = 9,
+    CNT_N = 16
 };
+
+// Kernel classes of pgpu_stats.kernel_ms.
+enum KernelClass { KC_GENERATE = 0, KC_EXTEND, KC_SHADE, KC_SHADOW, KC_ACCUMULATE, KC_MEGAKERNEL, KC_N };
 
 }  // namespace pgpu

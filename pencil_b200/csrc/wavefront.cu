@@ -93,8 +93,10 @@ __device__ __forceinline__ int find_job_pix(const WfJob* jobs, int n, long long 
     return lo;
 }
 
+// Add this thread's counters to the device totals (one atomic per warp and
+// counter). cls 1: traversal by extend, 2: by shadow (split node counters).
 template <bool COUNT>
-__device__ __forceinline__ void flush_counts(const WfArgs& A, const RayCount& rc) {
+__device__ __forceinline__ void flush_counts(const WfArgs& A, const RayCount& rc, int cls = 0) {
     if (!COUNT) return;
     unsigned long long v[6] = {rc.ext, rc.shadow, rc.ref, rc.tc.nodes, rc.tc.leaf_bytes,
                                rc.tc.prims};
@@ -102,7 +104,13 @@ __device__ __forceinline__ void flush_counts(const WfArgs& A, const RayCount& rc
     for (int k = 0; k < 6; ++k) {
         unsigned long long x = v[k];
         for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
-        if ((threadIdx.x & 31) == 0 && x) atomicAdd(A.counters + k, x);
+        if ((threadIdx.x & 31) == 0 && x) {
+            atomicAdd(A.counters + k, x);
+            if (cls == 1 && k == 3) atomicAdd(A.counters + CNT_NODES_EXT, x);
+            if (cls == 1 && k == 4) atomicAdd(A.counters + CNT_LEAF_EXT, x);
+            if (cls == 2 && k == 3) atomicAdd(A.counters + CNT_NODES_SH, x);
+            if (cls == 2 && k == 4) atomicAdd(A.counters + CNT_LEAF_SH, x);
+        }
     }
 }
 
@@ -213,7 +221,7 @@ wf_extend(WfArgs A, int it) {
             A.hit[slot] = make_float4(tb, __int_as_float(bref), __int_as_float(leaf), 0.0f);
         }
     }
-    flush_counts<COUNT>(A, rc);
+    flush_counts<COUNT>(A, rc, 1);
 }
 
 // ---- shade --------------------------------------------------------------------
@@ -362,7 +370,7 @@ wf_shadow(WfArgs A, int it) {
             }
         }
     }
-    flush_counts<COUNT>(A, rc);
+    flush_counts<COUNT>(A, rc, 2);
 }
 
 // ---- accumulate -----------------------------------------------------------------
@@ -533,9 +541,35 @@ static cudaError_t occupancy(WfOccupancy& o) {
 
 // Enqueue the kernels of the whole path space on `st` (captured into a graph
 // by the caller).
+// Events around launches when a render is profiled (kernel class, start, end).
+struct LaunchTimer {
+    bool on = false;
+    std::vector<int> cls;
+    std::vector<cudaEvent_t> ev;
+    void mark(int c, cudaStream_t st, bool start) {
+        if (!on) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        ev.push_back(e);
+        if (start) cls.push_back(c);
+    }
+    // sum per class after the stream has finished; releases the events
+    void collect(double* ms) {
+        for (size_t k = 0; k < cls.size(); ++k) {
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]);
+            ms[cls[k]] += t;
+        }
+        for (auto e : ev) cudaEventDestroy(e);
+        ev.clear();
+        cls.clear();
+    }
+};
+
 template <bool COUNT>
 static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& jobs, int iters,
-                                 int Qeff, cudaStream_t st, int* launches) {
+                                 int Qeff, cudaStream_t st, int* launches, LaunchTimer& lt) {
     WfOccupancy occ;
     cudaError_t e = occupancy<COUNT>(occ);
     if (e != cudaSuccess) return e;
@@ -566,16 +600,26 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         if ((e = cudaMemsetAsync(A.counts, 0, cnt_bytes, st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(A.work, 0, (size_t)(iters + 2) * 3 * 4, st)) != cudaSuccess) return e;
         int gblocks = (int)((slots + kWfBlock - 1) / kWfBlock);
+        lt.mark(KC_GENERATE, st, true);
         wf_generate<COUNT><<<gblocks, kWfBlock, 0, st>>>(A, path_begin, (int)slots);
+        lt.mark(KC_GENERATE, st, false);
         n_launch += 1;
         for (int it = 0; it < iters; ++it) {
+            lt.mark(KC_EXTEND, st, true);
             wf_extend<COUNT><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
+            lt.mark(KC_EXTEND, st, false);
+            lt.mark(KC_SHADE, st, true);
             wf_shade<COUNT><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
+            lt.mark(KC_SHADE, st, false);
+            lt.mark(KC_SHADOW, st, true);
             wf_shadow<COUNT><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
+            lt.mark(KC_SHADOW, st, false);
             n_launch += 3;
         }
         int ablocks = (int)((pixels + kWfBlock - 1) / kWfBlock);
+        lt.mark(KC_ACCUMULATE, st, true);
         wf_accumulate<<<ablocks, kWfBlock, 0, st>>>(A, pix_begin, (int)pixels, path_begin);
+        lt.mark(KC_ACCUMULATE, st, false);
         n_launch += 1;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
@@ -590,7 +634,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
                              const std::vector<int>& job_view, const std::vector<RenderCfg>& cfgs,
                              const std::vector<float*>& outs, const std::vector<float*>& m2s,
                              unsigned long long* counters, cudaStream_t st, bool use_graph,
-                             int* launches, int* status_out) {
+                             int* launches, int* status_out, double* kernel_ms) {
     const int n = (int)cfgs.size();
     std::vector<WfJob> jobs(n);
     long long path_off = 0, pix_off = 0;
@@ -650,14 +694,17 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     }
     mix((unsigned long long)iters);
     int nl = 0;
+    LaunchTimer lt;
+    lt.on = kernel_ms != nullptr;
+    if (lt.on) use_graph = false;
     if (use_graph) {
         if (!W.graph || W.graph_key != key) {
             if (W.graph) { cudaGraphExecDestroy(W.graph); W.graph = nullptr; }
             cudaGraph_t g = nullptr;
             if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
                 return e;
-            cudaError_t ee = count ? enqueue_frame<true>(W, jobs, iters, (int)Q, st, &nl)
-                                   : enqueue_frame<false>(W, jobs, iters, (int)Q, st, &nl);
+            cudaError_t ee = count ? enqueue_frame<true>(W, jobs, iters, (int)Q, st, &nl, lt)
+                                   : enqueue_frame<false>(W, jobs, iters, (int)Q, st, &nl, lt);
             e = cudaStreamEndCapture(st, &g);
             if (ee != cudaSuccess) { if (g) cudaGraphDestroy(g); return ee; }
             if (e != cudaSuccess) return e;
@@ -669,10 +716,14 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
         if ((e = cudaGraphLaunch(W.graph, st)) != cudaSuccess) return e;
         if (launches) *launches = 1;
     } else {
-        e = count ? enqueue_frame<true>(W, jobs, iters, (int)Q, st, &nl)
-                  : enqueue_frame<false>(W, jobs, iters, (int)Q, st, &nl);
+        e = count ? enqueue_frame<true>(W, jobs, iters, (int)Q, st, &nl, lt)
+                  : enqueue_frame<false>(W, jobs, iters, (int)Q, st, &nl, lt);
         if (e != cudaSuccess) return e;
         if (launches) *launches = nl;
+        if (lt.on) {
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+            lt.collect(kernel_ms);
+        }
     }
     if (status_out) {
         if ((e = cudaMemcpyAsync(status_out, W.args.status, 4, cudaMemcpyDeviceToHost, st)) !=

@@ -42,6 +42,7 @@ class RenderSettings:
     count_rays: bool = False
     count_nodes: bool = False
     use_graph: bool = True
+    profile_kernels: bool = False
     queue_capacity: int = 0
     sort_key: int = 0
 
@@ -57,7 +58,8 @@ class RenderSettings:
         p.sample_offset = self.sample_offset
         p.flags = ((A.FLAG_COUNT_RAYS if self.count_rays else 0) |
                    (A.FLAG_COUNT_NODES if self.count_nodes else 0) |
-                   (0 if self.use_graph else A.FLAG_NO_GRAPH))
+                   (0 if self.use_graph else A.FLAG_NO_GRAPH) |
+                   (A.FLAG_PROFILE_KERNELS if self.profile_kernels else 0))
         p.queue_capacity, p.sort_key = self.queue_capacity, self.sort_key
         return p
 
@@ -71,15 +73,23 @@ class RenderStats:
     shadow_rays: int = 0
     node_visits: int = 0
     prim_tests: int = 0
+    ext_node_visits: int = 0
+    ext_leaf_bytes: int = 0
+    shadow_node_visits: int = 0
+    shadow_leaf_bytes: int = 0
     device_ms: float = 0.0
     total_ms: float = 0.0
+    kernel_ms: dict = field(default_factory=dict)
     kernel_launches: int = 0
 
     def fill(self, s: A.Stats) -> None:
         self.rays_traced = s.reference_rays
         self.paths, self.extension_rays, self.shadow_rays = s.paths, s.extension_rays, s.shadow_rays
         self.node_visits, self.prim_tests = s.node_visits, s.prim_tests
+        self.ext_node_visits, self.ext_leaf_bytes = s.ext_node_visits, s.ext_leaf_bytes
+        self.shadow_node_visits, self.shadow_leaf_bytes = s.shadow_node_visits, s.shadow_leaf_bytes
         self.device_ms, self.total_ms = s.device_ms, s.total_ms
+        self.kernel_ms = dict(zip(A.KERNEL_CLASSES, list(s.kernel_ms)))
         self.kernel_launches = s.kernel_launches
 
 

@@ -1,0 +1,283 @@
+"""GPU core against the oracle and the reference fixtures, through the C-ABI.
+
+Bars:
+  * primary-hit / closest-hit primitive ids bit-exact, hit distances bit-exact
+    against the reference's float32 arithmetic and within 1e-5 relative of an
+    FP64 recomputation;
+  * the megakernel with Pencil's per-pixel RNG and two-branch glass equals the
+    reference image up to last-bit differences of libm's cos/sin/pow (at most
+    0.5% of pixel channels above 1e-4 relative);
+  * the wavefront engine equals the megakernel bit for bit;
+  * counter-RNG renders match the reference expectation within 3 sigma of the
+    Monte Carlo standard error per channel (aggregate: at most 1.5% of
+    channels beyond 3 sigma, image mean within 3 sigma).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_SCENES, load_golden
+from oracle import oracle as O
+from pencil_b200 import _abi as A
+from pencil_b200 import workloads as W
+from pencil_b200.renderer import RenderSettings, RenderStats
+from pencil_b200.scene import CameraArgs, Light, Material, Scene
+
+pytestmark = pytest.mark.gpu
+
+
+def settings_of(fx, pathtrace: bool, **kw) -> RenderSettings:
+    w, h, n, depth = (int(x) for x in fx["settings"])
+    return RenderSettings(width=w, height=h, samples=n, max_depth=depth, pathtrace=pathtrace,
+                          pathtrace_bounces=depth, **kw)
+
+
+def exact_mode(st: RenderSettings) -> RenderSettings:
+    st.engine, st.rng, st.glass = A.ENGINE_MEGAKERNEL, A.RNG_PIXEL_SEQUENTIAL, A.GLASS_BOTH_BRANCHES
+    return st
+
+
+def zscores(mu_a, m2_a, n_a, mu_b, m2_b, n_b):
+    va = np.maximum(m2_a.astype(np.float64) - mu_a.astype(np.float64) ** 2, 0) * n_a / (n_a - 1)
+    vb = np.maximum(m2_b.astype(np.float64) - mu_b.astype(np.float64) ** 2, 0) * n_b / (n_b - 1)
+    se = np.sqrt(va / n_a + vb / n_b)
+    diff = mu_a.astype(np.float64) - mu_b.astype(np.float64)
+    tol = 1e-5 * np.maximum(np.abs(mu_b), 1e-3)
+    z = np.where(se > 0, diff / np.maximum(se, 1e-30), np.where(np.abs(diff) <= tol, 0.0, np.inf))
+    return z, diff, se
+
+
+@pytest.fixture(scope="module")
+def scenes(gpu):
+    out = {}
+    for name in GOLDEN_SCENES:
+        scene, fx = load_golden(name)
+        sid = gpu.upload(scene, fx["nodes"])
+        out[name] = (scene, fx, sid)
+    return out
+
+
+@pytest.mark.parametrize("name", GOLDEN_SCENES)
+def test_closest_hits_bit_exact(gpu, scenes, name):
+    scene, fx, sid = scenes[name]
+    prim, t = gpu.trace_rays(sid, fx["rays"])
+    assert np.array_equal(prim, fx["hit_prim"])
+    assert np.array_equal(t.view(np.uint32), fx["hit_t"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", GOLDEN_SCENES)
+def test_primary_hits_bit_exact_and_fp64(gpu, scenes, name):
+    scene, fx, sid = scenes[name]
+    orc = O.Oracle(scene, fx["nodes"], fx["prims"])
+    rng = np.random.default_rng(7)
+    uv = np.concatenate([fx["uv"], rng.uniform(0, 1, (20000, 2))]).astype(np.float32)
+    prim, t = gpu.primary_hits(sid, uv)
+    op, ot = orc.primary_hits(uv)
+    assert np.array_equal(prim, op)
+    assert np.array_equal(t.view(np.uint32), ot.view(np.uint32))
+    rays = orc.camera_rays(uv)
+    hit = np.nonzero(prim >= 0)[0]
+    assert len(hit) > 0
+    sel = hit[:: max(1, len(hit) // 3000)]
+    t64 = np.array([orc.hit_t_fp64(int(prim[k]), rays[k]) for k in sel])
+    ok = t64 > 0
+    rel = np.abs(t[sel][ok] - t64[ok]) / t64[ok]
+    assert ok.mean() > 0.99
+    assert rel.max() < 1e-5
+
+
+@pytest.mark.parametrize("name", GOLDEN_SCENES)
+@pytest.mark.parametrize("mode", ["pt", "wh"])
+def test_megakernel_reference_rng_matches_reference(gpu, scenes, name, mode):
+    scene, fx, sid = scenes[name]
+    st = exact_mode(settings_of(fx, mode == "pt"))
+    img = gpu.render(sid, st)
+    ref = fx[f"hdr_{mode}"]
+    rel = np.abs(img.astype(np.float64) - ref) / np.maximum(np.abs(ref), 1e-3)
+    assert np.isfinite(img).all()
+    assert (rel > 1e-4).mean() <= 0.005
+    assert abs(img.mean() - ref.mean()) <= 1e-4 * max(ref.mean(), 1e-3)
+
+
+@pytest.mark.parametrize("name", GOLDEN_SCENES)
+@pytest.mark.parametrize("mode", ["pt", "wh"])
+def test_wavefront_equals_megakernel(gpu, scenes, name, mode):
+    scene, fx, sid = scenes[name]
+    st = settings_of(fx, mode == "pt", engine=A.ENGINE_MEGAKERNEL, count_rays=True)
+    s1, s2 = RenderStats(), RenderStats()
+    mk = gpu.render(sid, st, stats=s1)
+    st.engine = A.ENGINE_WAVEFRONT
+    wf = gpu.render(sid, st, stats=s2)
+    assert np.array_equal(mk.view(np.uint32), wf.view(np.uint32))
+    assert (s1.extension_rays, s1.shadow_rays) == (s2.extension_rays, s2.shadow_rays)
+    st.sort_key = 1
+    wf2 = gpu.render(sid, st)
+    assert np.array_equal(mk.view(np.uint32), wf2.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["c1", "cloud2k", "prims_mix", "cornell_box", "mesh_small"])
+@pytest.mark.parametrize("mode", ["pt", "wh"])
+def test_counter_rng_three_sigma(gpu, scenes, name, mode):
+    """Counter RNG + Fresnel-split glass (the production estimator) against
+    the reference algorithm's expectation (the oracle, bit-exact with the
+    reference), both at 64 samples per pixel."""
+    scene, fx, sid = scenes[name]
+    st = settings_of(fx, mode == "pt")
+    st.samples = 8
+    n = 64
+    mu_o, m2_o, _ = O.Oracle(scene, fx["nodes"], fx["prims"]).render(st, want_m2=True)
+    m2_g = np.zeros_like(mu_o)
+    mu_g = gpu.render(sid, st, m2=m2_g)
+    z, diff, se = zscores(mu_g, m2_g, n, mu_o, m2_o, n)
+    assert np.isfinite(mu_g).all()
+    frac = (np.abs(z) > 3).mean()
+    assert frac <= 0.015, f"{frac:.4f} of channels beyond 3 sigma"
+    img_se = np.sqrt((se ** 2).sum()) / se.size
+    assert abs(diff.mean()) <= 3 * img_se + 1e-7
+
+
+def test_quad_light_nee_matches_bsdf_only_reference(gpu):
+    """Area-light NEE (a quad light on the emissive ceiling quad) against
+    Pencil's estimator, which reaches the emitter by BSDF sampling only."""
+    w = W.mesh_box(subdiv=2, width=24, height=24, samples=16, depth=6)
+    scene = w.scene
+    sid = gpu.upload(scene)
+    st = w.settings
+    m2_g = np.zeros((24, 24, 3), np.float32)
+    mu_g = gpu.render(sid, st, m2=m2_g)
+    # the oracle, like Pencil, has no quad lights: it skips them
+    mu_o, m2_o, _ = O.Oracle(scene).render(st, want_m2=True)
+    z, diff, se = zscores(mu_g, m2_g, 256, mu_o, m2_o, 256)
+    assert (np.abs(z) > 3).mean() <= 0.02
+    img_se = np.sqrt((se ** 2).sum()) / se.size
+    assert abs(diff.mean()) <= 3 * img_se
+    # NEE lowers the variance of the estimate
+    var_g = np.maximum(m2_g - mu_g ** 2, 0).mean()
+    var_o = np.maximum(m2_o - mu_o ** 2, 0).mean()
+    assert var_g < var_o
+    gpu.free(sid)
+
+
+def test_batch_equals_individual_renders(gpu):
+    jobs = W.sphere_batch(n_scenes=6, seed=21)
+    sids = [gpu.upload(j.scene) for j in jobs]
+    sts = [j.settings for j in jobs]
+    for st in sts:
+        st.width = st.height = min(st.width, 96)
+    singles = [gpu.render(s, st) for s, st in zip(sids, sts)]
+    batch = gpu.render_batch(sids, sts)
+    for a, b in zip(singles, batch):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    for s in sids:
+        gpu.free(s)
+
+
+def test_renders_are_deterministic(gpu, scenes):
+    scene, fx, sid = scenes["prims_mix"]
+    for eng in (A.ENGINE_MEGAKERNEL, A.ENGINE_WAVEFRONT):
+        st = settings_of(fx, True, engine=eng)
+        a = gpu.render(sid, st)
+        b = gpu.render(sid, st)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        st.sample_offset = 4
+        c = gpu.render(sid, st)
+        assert not np.array_equal(a, c)
+
+
+def test_edge_cases(gpu):
+    # empty scene: background everywhere
+    s = Scene()
+    s.background = (0.25, 0.5, 0.75)
+    s.camera = CameraArgs(aspect=1.0)
+    sid = gpu.upload(s)
+    for eng in (A.ENGINE_MEGAKERNEL, A.ENGINE_WAVEFRONT):
+        img = gpu.render(sid, RenderSettings(width=7, height=5, samples=1, pathtrace=True,
+                                             pathtrace_bounces=3, engine=eng))
+        assert np.allclose(img, [0.25, 0.5, 0.75])
+        # depth 0: nothing traced, black
+        img = gpu.render(sid, RenderSettings(width=3, height=3, samples=2, pathtrace=True,
+                                             pathtrace_bounces=0, engine=eng))
+        assert np.all(img == 0)
+    gpu.free(sid)
+    # one primitive, 1x1 image, n = 1, odd n
+    s = Scene()
+    m = s.add_material(Material.diffuse((0.5, 0.5, 0.5)))
+    s.add_sphere((0, 0, 0), 1.0, m)
+    s.add_light(Light.point((0, 5, -5), (1, 1, 1)))
+    s.camera = CameraArgs((0, 0, -5), (0, 0, 0), (0, 1, 0), 30.0, 1.0)
+    sid = gpu.upload(s)
+    for n in (1, 3):
+        st = RenderSettings(width=1, height=1, samples=n, pathtrace=True, pathtrace_bounces=4)
+        a = gpu.render(sid, st)
+        st.engine = A.ENGINE_MEGAKERNEL
+        b = gpu.render(sid, st)
+        assert np.array_equal(a, b) and a.sum() > 0
+    gpu.free(sid)
+
+
+def test_invalid_arguments_return_status(gpu):
+    s = Scene()
+    m = s.add_material(Material.diffuse((0.5, 0.5, 0.5)))
+    s.add_sphere((0, 0, 0), 1.0, m)
+    sid = gpu.upload(s)
+    bad = [RenderSettings(width=0, height=4), RenderSettings(width=4, height=4, samples=0),
+           RenderSettings(width=4, height=4, samples=100)]
+    for st in bad:
+        with pytest.raises(A.GpuError) as e:
+            gpu.render(sid, st)
+        assert e.value.code == A.ERR_INVALID_ARG
+    with pytest.raises(A.GpuError) as e:
+        gpu.render(sid, RenderSettings(width=4, height=4, rng=A.RNG_PIXEL_SEQUENTIAL))
+    assert e.value.code == A.ERR_UNSUPPORTED
+    with pytest.raises(A.GpuError) as e:
+        gpu.render(9999, RenderSettings(width=4, height=4))
+    assert e.value.code == A.ERR_NO_SCENE
+    # a node table that is not Pencil's DFS order
+    nodes, _ = s.build_bvh()
+    s.add_sphere((3, 0, 0), 1.0, m)
+    nodes, _ = s.build_bvh()
+    broken = nodes.copy()
+    broken[0]["right"] = 1
+    with pytest.raises(A.GpuError) as e:
+        gpu.upload(s, broken)
+    assert e.value.code == A.ERR_BVH_INVALID
+    s.camera = CameraArgs(aperture=0.1)
+    with pytest.raises(A.GpuError) as e:
+        gpu.upload(s)
+    assert e.value.code == A.ERR_UNSUPPORTED
+    gpu.free(sid)
+
+
+def test_full_size_sphere_cloud_properties(gpu):
+    """The benchmark workload at full size (1280x720, 16 spp, 100k spheres):
+    size-independent properties -- both engines agree bit for bit, the image
+    is finite and non-negative, and primary hits agree with the oracle."""
+    w = W.sphere_cloud()
+    sid = gpu.upload(w.scene)
+    st = w.settings
+    st.engine = A.ENGINE_WAVEFRONT
+    wf = gpu.render(sid, st)
+    st.engine = A.ENGINE_MEGAKERNEL
+    mk = gpu.render(sid, st)
+    assert np.array_equal(wf.view(np.uint32), mk.view(np.uint32))
+    assert np.isfinite(wf).all() and (wf >= 0).all()
+    orc = O.Oracle(w.scene)
+    uv = np.random.default_rng(3).uniform(0, 1, (50000, 2)).astype(np.float32)
+    p, t = gpu.primary_hits(sid, uv)
+    op, ot = orc.primary_hits(uv)
+    assert np.array_equal(p, op) and np.array_equal(t.view(np.uint32), ot.view(np.uint32))
+    gpu.free(sid)
+
+
+def test_full_size_mesh_primary_hits(gpu):
+    """1,310,720-triangle indexed mesh (float32 vertices, int32 indices)."""
+    w = W.mesh_box()
+    sid = gpu.upload(w.scene)
+    orc = O.Oracle(w.scene)
+    uv = np.random.default_rng(4).uniform(0, 1, (20000, 2)).astype(np.float32)
+    p, t = gpu.primary_hits(sid, uv)
+    op, ot = orc.primary_hits(uv)
+    assert np.array_equal(p, op) and np.array_equal(t.view(np.uint32), ot.view(np.uint32))
+    assert (p >= w.scene.n_prims).mean() > 0.2       # rays that hit the mesh
+    gpu.free(sid)
