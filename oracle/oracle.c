@@ -676,6 +676,342 @@ int32_t orc_render(const orc_scene* s, const pgpu_render_params* p, float* out_r
     return 0;
 }
 
+/* ---- the GPU core's single-ray estimator, restated ---------------------------
+ * Test-only restatement of pencil_b200/csrc/path.cuh (shade_vertex, NeeAccum)
+ * and of the megakernel's per-pixel accumulation: counter RNG seeded by
+ * orc_path_seed, dielectric continuation along one Fresnel-chosen branch,
+ * quad-light NEE at diffuse vertices with the emitter's emission skipped on
+ * the following BSDF hit. Same float32 operation order as the device code,
+ * so GPU and oracle agree path for path up to libm's last bits. */
+enum { SPL_WHITTED = 1, SPL_SKIP_AREA = 2 };
+
+typedef struct {
+    int kind;          /* 0 none, 1 path-trace vertex, 2 Whitted vertex */
+    v3 local, contrib;
+} nee_acc;
+
+static void nee_add(nee_acc* a, v3* L, v3 c, int group_end, int visible) {
+    if (a->kind == 1) {
+        if (visible) *L = add(*L, c);
+    } else {
+        if (visible) a->contrib = add(a->contrib, c);
+        if (group_end > 0) {
+            a->local = add(a->local, divf(a->contrib, (float)group_end));
+            a->contrib = mk(0, 0, 0);
+        }
+    }
+}
+
+static void nee_finish(nee_acc* a, v3* L, v3 tail, v3 w, float sc) {
+    if (a->kind == 1) {
+        *L = add(*L, tail);
+    } else if (a->kind == 2) {
+        a->local = add(a->local, tail);
+        *L = add(*L, mulv(w, mulf(a->local, sc)));
+    }
+}
+
+static int quad_sample(const pgpu_light* l, float area, v3 p, v3 n, v3 sorg, float bias,
+                       rng_t* rng, v3* L, float* tmax, float* w) {
+    float u1 = rng_unit(rng);
+    float u2 = rng_unit(rng);
+    v3 y = add(add(ld3(l->pos), mulf(ld3(l->edge_u), u1)), mulf(ld3(l->edge_v), u2));
+    v3 d = sub(y, p);
+    float d2 = dot(d, d);
+    float dist = sqrtf(d2);
+    if (!(dist > 0.0f)) return 0;
+    *L = divf(d, dist);
+    float cx = dot(n, *L);
+    if (cx <= 0.0f) return 0;
+    v3 nq = nrm(cross(ld3(l->edge_u), ld3(l->edge_v)));
+    float ly = dot(nq, *L);
+    float cy = fabsf(ly);
+    *w = cx * cy * area / (3.14159265f * d2);
+    /* the biased shadow origin meets the emitter plane before |y - p|: test
+     * visibility up to that plane, never against the emitter itself */
+    *tmax = dot(sub(y, sorg), nq) / ly - bias;
+    return *w > 0.0f;
+}
+
+typedef struct {
+    ctx_t* c;
+    const char* area_emitter;   /* per material */
+    const float* quad_area;     /* per light */
+    int has_quad;
+} split_t;
+
+/* shade_vertex of path.cuh with every shadow ray resolved on the spot. */
+static int split_vertex(split_t* sp, ray_t* ray, v3* T, v3* L, rng_t* rng, int* depth,
+                        unsigned* flags, int found, const hitrec* h) {
+    ctx_t* c = sp->c;
+    const orc_scene* s = c->s;
+    const pgpu_render_params* P = c->p;
+    const int whitted = (*flags & SPL_WHITTED) != 0;
+    nee_acc acc;
+    acc.kind = 0;
+    v3 tail = mk(0, 0, 0), w = mk(0, 0, 0);
+    float sc = 0.0f;
+    int alive = 0;
+    if (!found) {
+        *L = add(*L, mulv(*T, ld3(s->background)));
+        return 0;
+    }
+    const pgpu_material* m = &s->materials[h->mat];
+    const v3 albedo = ld3(m->albedo);
+    const int metal = m->kind == PGPU_MAT_METAL && m->reflectivity > 0.0f;
+    const int glass = m->kind == PGPU_MAT_DIELECTRIC;
+    const v3 sorg = add(h->p, mulf(h->n, P->shadow_bias));
+    int dielectric = 0;
+    if (!whitted) {
+        const int diffuse = !metal && !glass;
+        if (!glass && !((*flags & SPL_SKIP_AREA) && sp->area_emitter[h->mat]))
+            *L = add(*L, mulv(*T, ld3(m->emission)));
+        acc.kind = 1;
+        for (int li = 0; li < s->n_lights; ++li) {
+            const pgpu_light* l = &s->lights[li];
+            if (l->kind == PGPU_LIGHT_QUAD) continue;
+            v3 Ld; float dist;
+            light_dir(l, h->p, rng, &Ld, &dist);
+            float ndotl = clampf(dot(h->n, Ld), 0.0f, 1.0f);
+            v3 cc = mulf(mulv(mulv(*T, albedo), ld3(l->intensity)), ndotl);
+            ray_t sr = {sorg, Ld};
+            int vis = l->is_emissive || !scene_occ(&c->tv, sr, P->shadow_bias, dist - P->shadow_bias);
+            nee_add(&acc, L, cc, 0, vis);
+        }
+        if (sp->has_quad && diffuse && *depth - 1 > 0) {
+            for (int li = 0; li < s->n_lights; ++li) {
+                const pgpu_light* l = &s->lights[li];
+                if (l->kind != PGPU_LIGHT_QUAD) continue;
+                v3 Ld; float tmax, wq;
+                if (!quad_sample(l, sp->quad_area[li], h->p, h->n, sorg, P->shadow_bias, rng,
+                                 &Ld, &tmax, &wq)) continue;
+                v3 cc = mulf(mulv(mulv(*T, albedo), ld3(l->intensity)), wq);
+                ray_t sr = {sorg, Ld};
+                int vis = !scene_occ(&c->tv, sr, P->shadow_bias, tmax);
+                nee_add(&acc, L, cc, 0, vis);
+            }
+        }
+        tail = mulv(mulv(*T, albedo), ld3(s->ambient));
+        if (P->depth - *depth > 3) {
+            float pr = fmaxf(T->x, fmaxf(T->y, T->z));
+            if (rng_unit(rng) > pr) { nee_finish(&acc, L, tail, w, sc); return 0; }
+            *T = divf(*T, pr);
+        }
+        if (!glass) {
+            v3 nd;
+            if (metal) {
+                v3 refl = nrm(reflect(nrm(ray->d), h->n));
+                v3 upv = (fabsf(refl.y) < 0.9f) ? mk(0, 1, 0) : mk(1, 0, 0);
+                v3 t1 = nrm(cross(refl, upv));
+                v3 t2 = nrm(cross(refl, t1));
+                float r1 = rng_unit(rng) * 0.1f;
+                float r2 = rng_unit(rng) * 6.28f;
+                nd = nrm(add(add(refl, mulf(t1, r1 * cosf(r2))), mulf(t2, r1 * sinf(r2))));
+                *T = mulf(mulv(*T, albedo), m->reflectivity);
+            } else {
+                float r1 = rng_unit(rng) * 6.2831853f;
+                float r2 = rng_unit(rng);
+                float r2s = sqrtf(r2);
+                v3 N = h->n;
+                v3 upv = (fabsf(N.y) < 0.9f) ? mk(0, 1, 0) : mk(1, 0, 0);
+                v3 Tn = nrm(cross(upv, N));
+                v3 B = nrm(cross(N, Tn));
+                nd = nrm(add(add(mulf(mulf(Tn, cosf(r1)), r2s), mulf(mulf(B, sinf(r1)), r2s)),
+                             mulf(N, sqrtf(1.0f - r2))));
+                *T = mulv(*T, albedo);
+            }
+            *flags = (diffuse && sp->has_quad) ? SPL_SKIP_AREA : 0u;
+            ray->o = sorg;
+            ray->d = nd;
+            *depth -= 1;
+            alive = *depth > 0;
+        } else {
+            dielectric = 1;
+        }
+    } else {
+        if (glass) acc.kind = 0;
+        else { acc.kind = 2; acc.local = ld3(m->emission); acc.contrib = mk(0, 0, 0); }
+        for (int li = 0; li < s->n_lights; ++li) {
+            const pgpu_light* l = &s->lights[li];
+            if (l->kind == PGPU_LIGHT_QUAD) continue;
+            int ns = (l->radius > 0.0f) ? P->soft_shadow_samples : 1;
+            for (int k = 0; k < ns; ++k) {
+                v3 Ld; float dist;
+                light_dir(l, h->p, rng, &Ld, &dist);
+                if (glass) continue;
+                float ndotl = clampf(dot(h->n, Ld), 0.0f, 1.0f);
+                v3 cc = mulf(mulv(albedo, ld3(l->intensity)), ndotl);
+                if (m->specular > 0.0f && ndotl > 0.0f) {
+                    v3 V = neg(nrm(ray->d));
+                    v3 H = nrm(add(Ld, V));
+                    float ndoth = clampf(dot(h->n, H), 0.0f, 1.0f);
+                    float spec = powf(ndoth, m->shininess);
+                    cc = add(cc, mulf(mulv(ld3(m->specular_color), ld3(l->intensity)), spec * m->specular));
+                }
+                ray_t sr = {sorg, Ld};
+                int vis = l->is_emissive || !scene_occ(&c->tv, sr, P->shadow_bias, dist - P->shadow_bias);
+                nee_add(&acc, L, cc, k == ns - 1 ? ns : 0, vis);
+            }
+        }
+        if (!glass) {
+            tail = mulv(albedo, ld3(s->ambient));
+            w = *T;
+            if (metal) {
+                sc = 1.0f - m->reflectivity;
+                nee_finish(&acc, L, tail, w, sc);
+                *T = mulf(mulv(*T, albedo), m->reflectivity);
+                ray->o = sorg;
+                ray->d = nrm(reflect(nrm(ray->d), h->n));
+                *depth -= 1;
+                return *depth > 0;
+            }
+            nee_finish(&acc, L, tail, w, 1.0f);
+            return 0;
+        }
+        dielectric = 1;
+    }
+    nee_finish(&acc, L, tail, w, sc);
+    if (!dielectric) return alive;
+    {
+        /* trace_dielectric's branches (src/renderer.hpp:1582-1627) */
+        float safe = fmaxf(m->ior, 0.01f);
+        float eta = h->front ? (1.0f / safe) : safe;
+        v3 nd = nrm(ray->d);
+        float cos_i = fabsf(dot(nd, h->n));
+        float sin_t2 = eta * eta * (1.0f - cos_i * cos_i);
+        ray_t refl = {add(h->p, mulf(h->n, P->shadow_bias)), nrm(reflect(nd, h->n))};
+        int tir = sin_t2 > 1.0f;
+        float kr = 1.0f;
+        ray_t refr = refl;
+        if (!tir) {
+            float cos_t = sqrtf(1.0f - sin_t2);
+            refr.o = sub(h->p, mulf(h->n, P->shadow_bias));
+            refr.d = nrm(add(mulf(nd, eta), mulf(h->n, eta * cos_i - cos_t)));
+            kr = schlick(h->front ? cos_i : cos_t, eta);
+        }
+        if (tir || rng_unit(rng) < kr) *ray = refl;
+        else *ray = refr;
+        *T = mulv(*T, albedo);
+        *depth -= 1;
+        *flags = SPL_WHITTED;
+        return *depth > 0;
+    }
+}
+
+static v3 split_sample(split_t* sp, ray_t r, rng_t* rng) {
+    ctx_t* c = sp->c;
+    v3 T = mk(1, 1, 1), L = mk(0, 0, 0);
+    int depth = c->p->depth;
+    unsigned flags = c->p->mode == PGPU_MODE_WHITTED ? SPL_WHITTED : 0u;
+    if (c->cnt) c->cnt[ORC_CNT_REFERENCE_RAYS]++;
+    int alive = depth > 0;
+    while (alive) {
+        hitrec h;
+        int found = scene_hit(&c->tv, r, 1e-4f, 1e9f, &h);
+        alive = split_vertex(sp, &r, &T, &L, rng, &depth, &flags, found, &h);
+    }
+    return L;
+}
+
+typedef struct {
+    const orc_scene* s;
+    const pgpu_render_params* p;
+    float* out;
+    float* m2;
+    int row0, stride;
+    const char* area_emitter;
+    const float* quad_area;
+    int has_quad;
+    uint64_t cnt[ORC_CNT_N];
+} sjob_t;
+
+static void* split_thread(void* arg) {
+    sjob_t* jb = (sjob_t*)arg;
+    const pgpu_render_params* p = jb->p;
+    ctx_t c;
+    c.s = jb->s; c.p = p; c.cnt = jb->cnt; c.tv.s = jb->s; c.tv.cnt = jb->cnt;
+    split_t sp = {&c, jb->area_emitter, jb->quad_area, jb->has_quad};
+    const int W = p->width, H = p->height, n = p->samples, spp = n * n;
+    int G = 1;
+    while (G * 2 <= (spp < 32 ? spp : 32)) G *= 2;
+    for (int j = jb->row0; j < H; j += jb->stride) {
+        for (int i = 0; i < W; ++i) {
+            v3 acc[32], acc2[32];
+            for (int g = 0; g < G; ++g) {
+                acc[g] = mk(0, 0, 0);
+                acc2[g] = mk(0, 0, 0);
+                for (int smp = g; smp < spp; smp += G) {
+                    rng_t rng = {orc_path_seed(i, j, smp + p->sample_offset, p->seed)};
+                    float u = (i + ((smp % n) + 0.5f) / n) / (float)W;
+                    float v = 1.0f - (j + ((smp / n) + 0.5f) / n) / (float)H;
+                    u += rng_sym(&rng) * (0.5f / (W * n));
+                    v += rng_sym(&rng) * (0.5f / (H * n));
+                    v3 col = split_sample(&sp, camera_ray(jb->s, u, v), &rng);
+                    acc[g] = add(acc[g], col);
+                    acc2[g] = add(acc2[g], mulv(col, col));
+                }
+            }
+            for (int off = G >> 1; off > 0; off >>= 1)
+                for (int g = 0; g < off; ++g) {
+                    acc[g] = add(acc[g], acc[g + off]);
+                    acc2[g] = add(acc2[g], acc2[g + off]);
+                }
+            size_t o = ((size_t)j * W + i) * 3;
+            jb->out[o + 0] = acc[0].x / (float)spp;
+            jb->out[o + 1] = acc[0].y / (float)spp;
+            jb->out[o + 2] = acc[0].z / (float)spp;
+            if (jb->m2) {
+                jb->m2[o + 0] = acc2[0].x / (float)spp;
+                jb->m2[o + 1] = acc2[0].y / (float)spp;
+                jb->m2[o + 2] = acc2[0].z / (float)spp;
+            }
+        }
+    }
+    return NULL;
+}
+
+int32_t orc_render_split(const orc_scene* s, const pgpu_render_params* p, float* out_rgb,
+                         float* out_m2, int32_t n_threads, uint64_t* counters) {
+    if (!s || !p || !out_rgb || p->width <= 0 || p->height <= 0 || p->samples <= 0) return -1;
+    char* area_emitter = (char*)calloc((size_t)(s->n_materials > 0 ? s->n_materials : 1), 1);
+    float* quad_area = (float*)calloc((size_t)(s->n_lights > 0 ? s->n_lights : 1), sizeof(float));
+    int has_quad = 0;
+    for (int k = 0; k < s->n_lights; ++k) {
+        const pgpu_light* l = &s->lights[k];
+        if (l->kind != PGPU_LIGHT_QUAD) continue;
+        v3 cr = cross(ld3(l->edge_u), ld3(l->edge_v));
+        quad_area[k] = sqrtf(cr.x * cr.x + cr.y * cr.y + cr.z * cr.z);
+        if (l->material >= 0 && l->material < s->n_materials) area_emitter[l->material] = 1;
+        has_quad = 1;
+    }
+    if (n_threads < 1) n_threads = 1;
+    if (n_threads > p->height) n_threads = p->height;
+    sjob_t* jobs = (sjob_t*)calloc((size_t)n_threads, sizeof(sjob_t));
+    pthread_t* th = (pthread_t*)calloc((size_t)n_threads, sizeof(pthread_t));
+    char* live = (char*)calloc((size_t)n_threads, 1);
+    for (int k = 0; k < n_threads; ++k) {
+        sjob_t* jb = &jobs[k];
+        jb->s = s; jb->p = p; jb->out = out_rgb; jb->m2 = out_m2;
+        jb->row0 = k; jb->stride = n_threads;
+        jb->area_emitter = area_emitter; jb->quad_area = quad_area; jb->has_quad = has_quad;
+    }
+    for (int k = 1; k < n_threads; ++k)
+        live[k] = pthread_create(&th[k], NULL, split_thread, &jobs[k]) == 0;
+    split_thread(&jobs[0]);
+    for (int k = 1; k < n_threads; ++k) {
+        if (live[k]) pthread_join(th[k], NULL);
+        else split_thread(&jobs[k]);
+    }
+    if (counters)
+        for (int q = 0; q < ORC_CNT_N; ++q) {
+            uint64_t a = 0;
+            for (int k = 0; k < n_threads; ++k) a += jobs[k].cnt[q];
+            counters[q] = a;
+        }
+    free(live); free(jobs); free(th); free(area_emitter); free(quad_area);
+    return 0;
+}
+
 /* ---- ray queries ---------------------------------------------------------- */
 void orc_trace_rays(const orc_scene* s, const float* rays, int32_t n, int32_t* prim_id,
                     float* t, uint64_t* counters) {

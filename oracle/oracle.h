@@ -65,6 +65,13 @@ int32_t orc_render(const orc_scene* s, const pgpu_render_params* p,
                    float* out_rgb, float* out_m2, int32_t n_threads,
                    uint64_t* counters);
 
+/* The GPU core's production estimator restated on the CPU (test-only):
+ * counter RNG (orc_path_seed), one Fresnel-chosen dielectric branch,
+ * quad-light NEE; per-pixel sums in the GPU megakernel's lane order. */
+int32_t orc_render_split(const orc_scene* s, const pgpu_render_params* p,
+                         float* out_rgb, float* out_m2, int32_t n_threads,
+                         uint64_t* counters);
+
 /* Closest hit in the reference's traversal order (left subtree first,
  * t_max clipped by the left result), t_min 1e-4, t_max 1e9. */
 void orc_trace_rays(const orc_scene* s, const float* rays, int32_t n,

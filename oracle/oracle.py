@@ -55,6 +55,8 @@ def load():
     lib.orc_render.argtypes = [C.POINTER(OrcScene), C.POINTER(A.RenderParams), C.c_void_p,
                                C.c_void_p, C.c_int32, C.c_void_p]
     lib.orc_render.restype = C.c_int32
+    lib.orc_render_split.argtypes = lib.orc_render.argtypes
+    lib.orc_render_split.restype = C.c_int32
     lib.orc_trace_rays.argtypes = [C.POINTER(OrcScene), C.c_void_p, C.c_int32, C.c_void_p,
                                    C.c_void_p, C.c_void_p]
     lib.orc_primary_hits.argtypes = [C.POINTER(OrcScene), C.c_void_p, C.c_int32, C.c_void_p,
@@ -104,6 +106,19 @@ class Oracle:
                                  threads or os.cpu_count() or 1, A.ptr(cnt))
         if rc != 0:
             raise ValueError("orc_render rejected its arguments")
+        return out, m2, cnt
+
+    def render_split(self, settings, threads: int | None = None, want_m2: bool = False):
+        """The GPU core's production estimator (counter RNG, Fresnel-split
+        glass, quad-light NEE) restated on the CPU."""
+        p = settings.params()
+        out = np.zeros((settings.height, settings.width, 3), np.float32)
+        m2 = np.zeros_like(out) if want_m2 else None
+        cnt = np.zeros(5, np.uint64)
+        rc = self.lib.orc_render_split(C.byref(self.s), C.byref(p), A.ptr(out), A.ptr(m2),
+                                       threads or os.cpu_count() or 1, A.ptr(cnt))
+        if rc != 0:
+            raise ValueError("orc_render_split rejected its arguments")
         return out, m2, cnt
 
     def trace_rays(self, rays: np.ndarray, counters: bool = False):

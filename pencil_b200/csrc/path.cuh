@@ -102,23 +102,29 @@ __device__ __forceinline__ V3 diffuse_dir(V3 N, Rng& rng) {
     return normalized(T * cosf(r1) * r2s + B * sinf(r1) * r2s + N * sqrtf(1.0f - r2));
 }
 
-// Uniform point on a quad light and the unshadowed estimator weight
-// cos_x * cos_y * area / (pi * r^2); returns false when the light faces away.
-__device__ __forceinline__ bool quad_sample(const DevLight& l, V3 p, V3 n, Rng& rng, V3& L,
-                                            float& dist, float& w) {
+// Uniform point y on a quad light, the unshadowed estimator weight
+// cos_x * cos_y * area / (pi * r^2) seen from p, and the extent of the shadow
+// test: the shadow ray starts at the biased origin `sorg`, so it meets the
+// emitter's plane before |y - p|; visibility is tested up to that plane minus
+// the bias, never against the emitter itself. Returns false when the light
+// faces away.
+__device__ __forceinline__ bool quad_sample(const DevLight& l, V3 p, V3 n, V3 sorg, float bias,
+                                            Rng& rng, V3& L, float& tmax, float& w) {
     float u1 = rng.unit();
     float u2 = rng.unit();
     V3 y = ld3(l.pos) + ld3(l.edge_u) * u1 + ld3(l.edge_v) * u2;
     V3 d = y - p;
     float d2 = dot(d, d);
-    dist = sqrtf(d2);
+    float dist = sqrtf(d2);
     if (!(dist > 0.0f)) return false;
     L = d / dist;
     float cx = dot(n, L);
     if (cx <= 0.0f) return false;
     V3 nq = normalized(cross(ld3(l.edge_u), ld3(l.edge_v)));
-    float cy = fabsf(dot(nq, L));
+    float ly = dot(nq, L);
+    float cy = fabsf(ly);
     w = cx * cy * l.area / (3.14159265f * d2);
+    tmax = dot(y - sorg, nq) / ly - bias;
     return w > 0.0f;
 }
 
@@ -213,9 +219,9 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& S, const PathParam
                 const DevLight& l = S.lights[li];
                 if (l.kind != 2) continue;
                 V3 L;
-                float dist, w;
-                if (!quad_sample(l, h.p, h.n, ps.rng, L, dist, w)) continue;
-                E.shadow(ps.L, Ray{sorg, L}, P.bias, dist - P.bias, true,
+                float tmax, w;
+                if (!quad_sample(l, h.p, h.n, sorg, P.bias, ps.rng, L, tmax, w)) continue;
+                E.shadow(ps.L, Ray{sorg, L}, P.bias, tmax, true,
                          ps.T * albedo * ld3(l.intensity) * w, 0);
             }
         }
@@ -502,10 +508,11 @@ struct Tracer {
                 const DevLight& l = S.lights[li];
                 if (l.kind != 2) continue;
                 V3 L;
-                float dist, w;
-                if (!quad_sample(l, h.p, h.n, rng, L, dist, w)) continue;
-                Ray sr{h.p + h.n * P.bias, L};
-                if (occluded(sr, P.bias, dist - P.bias)) continue;
+                float tmax, w;
+                V3 sorg = h.p + h.n * P.bias;
+                if (!quad_sample(l, h.p, h.n, sorg, P.bias, rng, L, tmax, w)) continue;
+                Ray sr{sorg, L};
+                if (occluded(sr, P.bias, tmax)) continue;
                 rad = rad + T * albedo * ld3(l.intensity) * w;
             }
         }

@@ -296,10 +296,7 @@ wf_shade(WfArgs A, int it) {
             StoreNee E(A, slot);
             alive = shade_vertex(S, J.P, ps, found, h, E);
             E.store();
-            if (COUNT) {
-                rc.shadow += E.n;
-                if (alive && (ps.flags & kFlagWhitted)) rc.ref++;
-            }
+            if (COUNT && alive && (ps.flags & kFlagWhitted)) rc.ref++;
             A.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 0.0f);
             if (alive) {
                 A.ray_o[slot] = make_float4(ps.ray.o.x, ps.ray.o.y, ps.ray.o.z, 0.0f);
@@ -360,6 +357,7 @@ wf_shadow(WfArgs A, int it) {
                     int bits = __float_as_int(sc.w);
                     bool vis = true;
                     if (bits & 1) {
+                        if (COUNT) rc.shadow++;
                         Ray r{v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z)};
                         vis = !any_hit<kWfShared, COUNT>(S, r, so.w, sd.w, stk, &rc.tc);
                     }

@@ -7,8 +7,9 @@ No public dataset is involved: every scene is generated from a numpy seed.
   sphere_cloud       100,000 random spheres (60/30/10 diffuse/metal/glass), one
                      directional light, sky 0.3; 1280x720, n=4 (16 spp), depth 8
   mesh_box           displaced icosphere (8 subdivisions, 1,310,720 triangles,
-                     float32 vertices + int32 indices) in a 5-quad box with a
-                     0.25x0.25 emissive ceiling quad used as an area light;
+                     float32 vertices + int32 indices) in a box of 5 diffuse
+                     walls with a 0.25x0.25 emissive quad in the ceiling, used
+                     as an area light;
                      1024x1024, n=8 (64 spp), depth 12
   sphere_batch       256 sphere_cloud scenes of 10..50,000 spheres at
                      128/256/512 squared with 1/4/16/64 spp, depth 8
@@ -161,20 +162,26 @@ def value_noise(p: np.ndarray, seed: int, octaves: int = 3, base_freq: float = 2
 def _box(s: Scene, emitter_radiance=(17.0, 12.0, 4.0)) -> None:
     """Unit box [0,1]^3 open at z=0: floor, ceiling, back (albedo 0.75), red
     left wall and green right wall (0.65 in their own channel, 0.05 in the
-    others), and a 0.25 x 0.25 emissive ceiling quad used as a quad light."""
+    others). The ceiling is four quads around a 0.25 x 0.25 opening at its
+    centre, which the emissive quad fills (coplanar, facing down); that quad
+    is also registered as a quad light. Keeping the emitter in the ceiling
+    plane leaves no surface just above it, where the 1/r^2 of area sampling
+    would blow up."""
     white = s.add_material(Material.diffuse((0.75, 0.75, 0.75)))
     red = s.add_material(Material.diffuse((0.65, 0.05, 0.05)))
     green = s.add_material(Material.diffuse((0.05, 0.65, 0.05)))
     emit = s.add_material(Material.emissive(emitter_radiance))
+    c0, c1 = 0.375, 0.625
     s.add_quad((0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1), white)      # floor
-    s.add_quad((0, 1, 0), (0, 1, 1), (1, 1, 1), (1, 1, 0), white)      # ceiling
+    s.add_quad((0, 1, 0), (0, 1, 1), (c0, 1, 1), (c0, 1, 0), white)    # ceiling, left of the opening
+    s.add_quad((c1, 1, 0), (c1, 1, 1), (1, 1, 1), (1, 1, 0), white)    # right of it
+    s.add_quad((c0, 1, 0), (c0, 1, c0), (c1, 1, c0), (c1, 1, 0), white)  # in front of it
+    s.add_quad((c0, 1, c1), (c0, 1, 1), (c1, 1, 1), (c1, 1, c1), white)  # behind it
     s.add_quad((0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1), white)      # back
     s.add_quad((0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 0), red)        # left
     s.add_quad((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1), green)      # right
-    y = 0.999
-    c0, c1 = 0.375, 0.625
-    s.add_quad((c0, y, c0), (c0, y, c1), (c1, y, c1), (c1, y, c0), emit)
-    s.add_light(Light.quad((c0, y, c0), (0.25, 0, 0), (0, 0, 0.25), emitter_radiance, emit))
+    s.add_quad((c0, 1, c0), (c0, 1, c1), (c1, 1, c1), (c1, 1, c0), emit)
+    s.add_light(Light.quad((c0, 1, c0), (0.25, 0, 0), (0, 0, 0.25), emitter_radiance, emit))
     s.background = (0.0, 0.0, 0.0)
     s.ambient = (0.0, 0.0, 0.0)
 
