@@ -330,6 +330,38 @@ int32_t pgpu_adjoint(pgpu_ctx* ctx, int32_t scene_id,
                      double* d_albedo, double* d_emission, double* d_light,
                      float* out_rgb, pgpu_stats* stats);
 
+/* Render without allocating. No counterpart in the reference: Pencil renders
+ * on the CPU and never touches device memory.
+ *
+ * pgpu_render may allocate device memory on the way (its output staging and
+ * the wavefront's path queues grow with the image), and cudaMalloc/cudaFree
+ * synchronize the device. Some callers cannot allow that while a frame is in
+ * flight: a host whose device memory is owned by another allocator (a
+ * framework's caching allocator that has reserved the GPU), a real-time loop
+ * that must not stall on an allocation, or code that runs between
+ * allocation-free phases of a larger pipeline. This entry point renders with
+ * the wavefront engine over one file-scope device array of fixed size
+ * (21.5 MiB: 65,536 paths in flight, processed chunk after chunk; every GPU
+ * that loads the library holds it until exit). It calls no cudaMalloc,
+ * cudaFree or other allocating routine; the scene must already be uploaded
+ * and the outputs are caller-owned DEVICE buffers (out_rgb_device:
+ * width*height*3 floats; out_m2_device optional).
+ *
+ * Limits, rejected with PGPU_ERR_INVALID_ARG and a message: at most 4 shadow
+ * rays per path vertex (path-trace: one per light; Whitted: the soft-shadow
+ * samples of every light), depth <= 64, no ray counting, profiling or ray
+ * sorting. Counter RNG and Fresnel-split glass, as the wavefront engine.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and reserves the context's error-message buffer;
+ * make that first call before any stream capture. Every call shares the one
+ * array and leaves its contents behind (each call clears what it reads
+ * before it is written); calls that overlap on the GPU -- from two contexts
+ * or two streams at once -- race on it and must be serialized. */
+int32_t pgpu_render_noalloc(pgpu_ctx* ctx, int32_t scene_id,
+                            const pgpu_render_params* params,
+                            float* out_rgb_device, float* out_m2_device);
+
 /* Replace material table entries of an uploaded scene (same count), e.g.
  * between inverse-rendering steps. */
 int32_t pgpu_update_materials(pgpu_ctx* ctx, int32_t scene_id,

@@ -120,6 +120,8 @@ EXPORTS = {
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.POINTER(Stats)]),
     "pgpu_update_materials": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
+    "pgpu_render_noalloc": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(RenderParams),
+                                        C.c_void_p, C.c_void_p]),
 }
 
 _lib: C.CDLL | None = None

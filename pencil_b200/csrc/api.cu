@@ -33,6 +33,12 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
                              unsigned long long* counters, cudaStream_t st, bool use_graph,
                              int* launches, int* status_out, double* kernel_ms);
 
+cudaError_t wavefront_render_static(int device, const SceneView& view, const DevLight* lights,
+                                    int n_lights, bool has_glass, const RenderCfg& c, float* out,
+                                    float* m2, cudaStream_t st, int* status_host, int* launches,
+                                    const char** why);
+size_t static_scratch_bytes();
+
 constexpr int kMaxDepth = 64;          // traversal stack bound (kMaxStack)
 constexpr int kMaxTreeFrames = 32;     // Whitted recursion bound of the two-branch mode
 
@@ -861,3 +867,37 @@ int32_t pgpu_primary_hits(pgpu_ctx* c, int32_t id, const float* uv, int32_t n, i
 }
 
 }  // extern "C"
+
+// ---- render without allocating ------------------------------------------------------
+// For callers that must not allocate device memory while rendering (see
+// pencil_gpu.h). The first call on a device looks up the static scratch's
+// address and reserves the context's error-message buffer; after that no call
+// allocates host or device memory.
+extern "C" int32_t pgpu_render_noalloc(pgpu_ctx* c, int32_t id, const pgpu_render_params* p,
+                                       float* out_rgb_device, float* out_m2_device) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    if (c->err.capacity() < 512) c->err.reserve(512);
+    DeviceScene* ds = find_scene(c, id);
+    if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
+    if (!out_rgb_device) return fail(c, PGPU_ERR_INVALID_ARG, "null output");
+    RenderCfg cfg;
+    int rc = make_cfg(c, ds, p, cfg);
+    if (rc) return rc;
+    if (cfg.engine != PGPU_ENGINE_WAVEFRONT)
+        return fail(c, PGPU_ERR_UNSUPPORTED, "the no-allocation render is the wavefront engine");
+    PGPU_CUDA(c, cudaSetDevice(c->device));
+    const char* why = nullptr;
+    int launches = 0;
+    bool has_glass = false;
+    for (const auto& m : ds->mats) has_glass = has_glass || m.kind == PGPU_MAT_DIELECTRIC;
+    *c->h_status = 0;
+    cudaError_t e = wavefront_render_static(c->device, ds->view, ds->lights.data(),
+                                            (int)ds->lights.size(), has_glass, cfg, out_rgb_device,
+                                            out_m2_device, c->stream, c->h_status, &launches,
+                                            &why);
+    if (why) return fail(c, PGPU_ERR_INVALID_ARG, "%s", why);
+    if (e != cudaSuccess) return cuda_fail(c, e, "no-allocation render");
+    PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (*c->h_status != 0) return fail(c, PGPU_ERR_QUEUE_OVERFLOW, "shadow record overflow");
+    return PGPU_OK;
+}

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "host_internal.h"
@@ -745,6 +746,163 @@ void wavefront_delete(WfScratch* W) {
     if (!W) return;
     wavefront_release(*W);
     delete W;
+}
+
+}  // namespace pgpu
+
+// ---- rendering without allocating -------------------------------------------------
+// pgpu_render_noalloc: the same wavefront kernels driven over one statically
+// sized device array instead of context-owned scratch, for callers that may
+// not allocate device memory during a render. The array belongs to this
+// translation unit's module: every GPU that loads it holds it until exit.
+namespace pgpu {
+
+constexpr int kStaticSlots = 65536;       // paths in flight per chunk
+constexpr int kStaticShadow = 4;          // shadow records per vertex
+constexpr int kStaticMaxDepth = 64;       // bounces (iterations per chunk)
+constexpr size_t static_al(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t kStaticArray = static_al((size_t)kStaticSlots * 16);
+constexpr size_t kStaticBytes =
+    9 * kStaticArray +                                           // path state
+    3 * (size_t)kStaticShadow * kStaticArray +                   // shadow records
+    2 * static_al((size_t)kStaticSlots * 4) +                    // queues (one bin each)
+    static_al((size_t)(kStaticMaxDepth + 2) * kOctants * 4) +    // queue counts
+    static_al((size_t)(kStaticMaxDepth + 2) * 3 * 4) +           // fetch cursors
+    static_al(4) +                                               // status word
+    static_al(sizeof(SceneView)) + static_al(sizeof(WfJob));
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+size_t static_scratch_bytes() { return kStaticBytes; }
+
+// Device address of g_static_scratch on the current device, looked up once
+// per device (cudaGetSymbolAddress) and cached.
+static std::mutex g_static_mu;
+static void* g_static_ptr[64];
+
+cudaError_t static_scratch_address(int device, void** out) {
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    if (!g_static_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return e;
+        g_static_ptr[device] = p;
+    }
+    *out = g_static_ptr[device];
+    return cudaSuccess;
+}
+
+// Render one job over the static scratch. Returns cudaSuccess, or sets *why
+// (a constant string) and returns cudaErrorInvalidValue when the job exceeds
+// the scratch's fixed capacity. No allocation on the host or the device.
+cudaError_t wavefront_render_static(int device, const SceneView& view, const DevLight* lights,
+                                    int n_lights, bool has_glass, const RenderCfg& c, float* out,
+                                    float* m2, cudaStream_t st, int* status_host, int* launches,
+                                    const char** why) {
+    *why = nullptr;
+    // shadow records a vertex can make: path-trace vertices one per light;
+    // Whitted vertices (the Whitted mode, or after glass) the soft-shadow
+    // samples of every point/directional light
+    int pt = 0, wh = 0;
+    for (int k = 0; k < n_lights; ++k) {
+        pt += 1;
+        if (lights[k].kind != 2) wh += lights[k].radius > 0.0f ? c.soft : 1;
+    }
+    const bool whitted_vertices = c.mode == kModeWhitted || has_glass;
+    const int maxS = (whitted_vertices && wh > pt) ? wh : pt;
+    if (maxS > kStaticShadow) {
+        *why = "the scene needs more than 4 shadow rays per path vertex, the most the "
+               "no-allocation render holds";
+        return cudaErrorInvalidValue;
+    }
+    if (c.depth > kStaticMaxDepth) {
+        *why = "depth above 64 is beyond the no-allocation render";
+        return cudaErrorInvalidValue;
+    }
+    if (c.spp > kStaticSlots || c.sort_key != 0 || c.count || c.profile) {
+        *why = "the no-allocation render takes no ray sorting, counting or profiling";
+        return cudaErrorInvalidValue;
+    }
+    void* base = nullptr;
+    cudaError_t e = static_scratch_address(device, &base);
+    if (e != cudaSuccess) return e;
+    const int Q = kStaticSlots;
+    unsigned char* p = static_cast<unsigned char*>(base);
+    auto take = [&](size_t b) { unsigned char* r = p; p += static_al(b); return r; };
+    WfArgs A{};
+    A.n_jobs = 1;
+    A.Q = Q;
+    A.maxS = kStaticShadow;
+    A.ray_o = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.ray_d = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.T = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.L = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.st = reinterpret_cast<uint4*>(take((size_t)Q * 16));
+    A.hit = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.pb = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.pt = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.pw = reinterpret_cast<float4*>(take((size_t)Q * 16));
+    A.sh_o = reinterpret_cast<float4*>(take((size_t)kStaticShadow * Q * 16));
+    A.sh_d = reinterpret_cast<float4*>(take((size_t)kStaticShadow * Q * 16));
+    A.sh_c = reinterpret_cast<float4*>(take((size_t)kStaticShadow * Q * 16));
+    A.q[0] = reinterpret_cast<int*>(take((size_t)Q * 4));
+    A.q[1] = reinterpret_cast<int*>(take((size_t)Q * 4));
+    A.counts = reinterpret_cast<int*>(take((size_t)(kStaticMaxDepth + 2) * kOctants * 4));
+    A.work = reinterpret_cast<unsigned int*>(take((size_t)(kStaticMaxDepth + 2) * 3 * 4));
+    A.status = reinterpret_cast<int*>(take(4));
+    SceneView* d_view = reinterpret_cast<SceneView*>(take(sizeof(SceneView)));
+    WfJob* d_job = reinterpret_cast<WfJob*>(take(sizeof(WfJob)));
+    A.views = d_view;
+    A.jobs = d_job;
+    A.counters = nullptr;
+    A.sort_key = 0;
+    WfJob J;
+    J.P = PathParams{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias,
+                     c.salt, c.sample_offset};
+    J.view = 0;
+    J.path_off = 0;
+    J.pix_off = 0;
+    J.G = lanes_for(c.spp);
+    J.out = out;
+    J.m2 = m2;
+    // Every call shares the array: the tables are rewritten and the status
+    // word, queue counts and fetch cursors are cleared before they are read.
+    if ((e = cudaMemcpyAsync(d_view, &view, sizeof(SceneView), cudaMemcpyHostToDevice, st)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(d_job, &J, sizeof(WfJob), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemsetAsync(A.status, 0, 4, st)) != cudaSuccess) return e;
+    WfOccupancy occ;
+    if ((e = occupancy<false>(occ)) != cudaSuccess) return e;
+    const size_t smem = (size_t)kWfShared * kWfBlock * 8;
+    const long long npix = (long long)c.W * c.H;
+    const long long ppc = Q / c.spp;
+    int n_launch = 0;
+    for (long long pix0 = 0; pix0 < npix; pix0 += ppc) {
+        const long long pixels = (npix - pix0) < ppc ? (npix - pix0) : ppc;
+        const long long slots = pixels * c.spp;
+        const long long path0 = pix0 * c.spp;
+        if ((e = cudaMemsetAsync(A.counts, 0, (size_t)(c.depth + 2) * kOctants * 4, st)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaMemsetAsync(A.work, 0, (size_t)(c.depth + 2) * 3 * 4, st)) != cudaSuccess)
+            return e;
+        wf_generate<false><<<(unsigned)((slots + kWfBlock - 1) / kWfBlock), kWfBlock, 0, st>>>(
+            A, path0, (int)slots);
+        for (int it = 0; it < c.depth; ++it) {
+            wf_extend<false><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
+            wf_shade<false><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
+            wf_shadow<false><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
+        }
+        wf_accumulate<<<(unsigned)((pixels + kWfBlock - 1) / kWfBlock), kWfBlock, 0, st>>>(
+            A, pix0, (int)pixels, path0);
+        n_launch += 2 + 3 * c.depth;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (launches) *launches = n_launch;
+    return cudaMemcpyAsync(status_host, A.status, 4, cudaMemcpyDeviceToHost, st);
 }
 
 }  // namespace pgpu
