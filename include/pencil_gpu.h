@@ -226,7 +226,9 @@ typedef struct pgpu_render_params {
     int32_t  sample_offset;     /* first sample index (progressive renders)  */
     int32_t  flags;             /* enum pgpu_flags                           */
     int32_t  queue_capacity;    /* wavefront paths in flight (0: automatic)  */
-    int32_t  block_size;        /* threads per block (0: automatic)          */
+    int32_t  refill_below;      /* wavefront: a warp takes new rays once at
+                                   most this many of its 32 lanes are still
+                                   traversing (0: automatic)                 */
     int32_t  sort_key;          /* wavefront ray-sort key (0: none)          */
 } pgpu_render_params;
 

@@ -75,7 +75,7 @@ class RenderParams(C.Structure):
                 ("rng", C.c_int32), ("glass", C.c_int32), ("shadow_bias", C.c_float),
                 ("soft_shadow_samples", C.c_int32), ("seed", C.c_uint32),
                 ("sample_offset", C.c_int32), ("flags", C.c_int32),
-                ("queue_capacity", C.c_int32), ("block_size", C.c_int32),
+                ("queue_capacity", C.c_int32), ("refill_below", C.c_int32),
                 ("sort_key", C.c_int32)]
 
 

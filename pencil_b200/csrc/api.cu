@@ -631,7 +631,9 @@ int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, Re
     cfg.salt = p->seed;
     cfg.sample_offset = p->sample_offset;
     cfg.count = (p->flags & (PGPU_FLAG_COUNT_RAYS | PGPU_FLAG_COUNT_NODES)) != 0;
-    cfg.block = p->block_size;
+    if (p->refill_below < 0 || p->refill_below > 31)
+        return fail(c, PGPU_ERR_INVALID_ARG, "refill_below must be 0..31");
+    cfg.refill = p->refill_below;
     cfg.queue_capacity = p->queue_capacity;
     cfg.sort_key = p->sort_key;
     cfg.profile = (p->flags & PGPU_FLAG_PROFILE_KERNELS) != 0;

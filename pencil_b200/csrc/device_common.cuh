@@ -490,11 +490,160 @@ struct TravStack {
     }
 };
 
-// Closest hit: the primitive with the smallest t in [tmin, tmax]; among equal
-// t the one later in DFS leaf order wins, which is the primitive
-// BVHNode::hit (src/bvh.hpp:31-37) returns, since it visits leaves left to
-// right and accepts t <= t_max. Children are visited nearest first; the box
-// test itself is AABB::hit's arithmetic. Returns the leaf slot or -1.
+// Resumable closest-hit traversal: init() tests the root, step() processes
+// one interior node; both return true once the traversal has finished.
+// Result: the primitive with the smallest t in [tmin, tmax]; among equal t
+// the one later in DFS leaf order wins, which is the primitive BVHNode::hit
+// (src/bvh.hpp:31-37) returns, since it visits leaves left to right and
+// accepts t <= t_max. Children are visited nearest first; the box test is
+// AABB::hit's arithmetic. Split into steps so that a persistent kernel can
+// give a lane a new ray as soon as its old one finishes.
+template <int kShared, bool COUNT>
+struct ClosestTrav {
+    Ray ray;
+    RayPre rp;
+    float tmin, t_best;
+    int best, best_ref;
+    int node, sp;
+
+    __device__ __forceinline__ void test_leaf(const SceneView& S, int ref, TravCount* cnt) {
+        float t;
+        if (COUNT) { cnt->prims++; cnt->leaf_bytes += leaf_bytes(ref); }
+        if (hit_leaf<false>(S, ref, ray, tmin, t_best, t, nullptr)) {
+            int slot = (~ref) & kLeafSlotMask;
+            if (t < t_best || slot > best) { t_best = t; best = slot; best_ref = ref; }
+        }
+    }
+
+    __device__ __forceinline__ bool init(const SceneView& S, const Ray& r, float tmin_,
+                                         float tmax, TravCount* cnt) {
+        ray = r;
+        tmin = tmin_;
+        t_best = tmax;
+        best = -1;
+        best_ref = 0;
+        sp = 0;
+        node = 0;
+        if (S.root_ref == kEmptyRoot) return true;
+        rp = prep(r);
+        float e;
+        if (!slab(S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1],
+                  S.root_max[2], rp, tmin, tmax, e))
+            return true;
+        if (S.root_ref < 0) {
+            test_leaf(S, S.root_ref, cnt);
+            return true;
+        }
+        return false;
+    }
+
+    __device__ __forceinline__ bool step(const SceneView& S, TravStack<kShared>& stk,
+                                         TravCount* cnt) {
+        const float4* np = S.nodes + 4 * (size_t)node;
+        float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+        int4 rr = __ldg(reinterpret_cast<const int4*>(np + 3));
+        if (COUNT) cnt->nodes++;
+        float eL, eR;
+        bool hL = slab(a.x, a.y, a.z, a.w, b.x, b.y, rp, tmin, t_best, eL);
+        bool hR = slab(b.z, b.w, c.x, c.y, c.z, c.w, rp, tmin, t_best, eR);
+        if (hL && rr.x < 0) { test_leaf(S, rr.x, cnt); hL = false; }
+        if (hR && rr.y < 0) { if (eR <= t_best) test_leaf(S, rr.y, cnt); hR = false; }
+        hL = hL && eL <= t_best;
+        hR = hR && eR <= t_best;
+        if (hL && hR) {
+            if (eR < eL) { stk.push(sp, rr.x, eL); node = rr.y; }
+            else { stk.push(sp, rr.y, eR); node = rr.x; }
+            ++sp;
+            return false;
+        }
+        if (hL) { node = rr.x; return false; }
+        if (hR) { node = rr.y; return false; }
+        while (sp > 0) {
+            --sp;
+            int ref;
+            float te;
+            stk.pop(sp, ref, te);
+            if (te <= t_best) { node = ref; return false; }
+        }
+        return true;
+    }
+};
+
+// Resumable any-hit traversal (BVHNode::occluded, src/bvh.hpp:39-48). With a
+// fixed t_max the box test is order independent, so the answer equals the
+// reference's.
+template <int kShared, bool COUNT>
+struct AnyTrav {
+    Ray ray;
+    RayPre rp;
+    float tmin, tmax;
+    int node, sp;
+    bool hit;
+
+    __device__ __forceinline__ bool test_leaf(const SceneView& S, int ref, TravCount* cnt) {
+        float t;
+        if (COUNT) { cnt->prims++; cnt->leaf_bytes += leaf_bytes(ref); }
+        return hit_leaf<false>(S, ref, ray, tmin, tmax, t, nullptr);
+    }
+
+    __device__ __forceinline__ bool init(const SceneView& S, const Ray& r, float tmin_,
+                                         float tmax_, TravCount* cnt) {
+        ray = r;
+        tmin = tmin_;
+        tmax = tmax_;
+        hit = false;
+        sp = 0;
+        node = 0;
+        if (S.root_ref == kEmptyRoot) return true;
+        rp = prep(r);
+        float e;
+        if (!slab(S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1],
+                  S.root_max[2], rp, tmin, tmax, e))
+            return true;
+        if (S.root_ref < 0) {
+            hit = test_leaf(S, S.root_ref, cnt);
+            return true;
+        }
+        return false;
+    }
+
+    __device__ __forceinline__ bool step(const SceneView& S, TravStack<kShared>& stk,
+                                         TravCount* cnt) {
+        const float4* np = S.nodes + 4 * (size_t)node;
+        float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+        int4 rr = __ldg(reinterpret_cast<const int4*>(np + 3));
+        if (COUNT) cnt->nodes++;
+        float eL, eR;
+        bool hL = slab(a.x, a.y, a.z, a.w, b.x, b.y, rp, tmin, tmax, eL);
+        bool hR = slab(b.z, b.w, c.x, c.y, c.z, c.w, rp, tmin, tmax, eR);
+        if (hL && rr.x < 0) {
+            if (test_leaf(S, rr.x, cnt)) { hit = true; return true; }
+            hL = false;
+        }
+        if (hR && rr.y < 0) {
+            if (test_leaf(S, rr.y, cnt)) { hit = true; return true; }
+            hR = false;
+        }
+        if (hL && hR) {
+            if (eR < eL) { stk.push(sp, rr.x, 0.0f); node = rr.y; }
+            else { stk.push(sp, rr.y, 0.0f); node = rr.x; }
+            ++sp;
+            return false;
+        }
+        if (hL) { node = rr.x; return false; }
+        if (hR) { node = rr.y; return false; }
+        if (sp == 0) return true;
+        --sp;
+        float te;
+        stk.pop(sp, node, te);
+        return false;
+    }
+};
+
+// Closest hit of one ray, traced to the end in one loop (megakernel,
+// queries): the same traversal as ClosestTrav, written as a single loop,
+// which compiles to fewer registers inside the megakernel. Returns the leaf
+// slot or -1.
 template <int kShared, bool COUNT>
 __device__ int closest_hit(const SceneView& S, const Ray& ray, float tmin, float tmax,
                            float& t_best, int& best_ref, TravStack<kShared>& stk,
@@ -532,7 +681,8 @@ __device__ int closest_hit(const SceneView& S, const Ray& ray, float tmin, float
         bool hR = slab(b.z, b.w, c.x, c.y, c.z, c.w, rp, tmin, t_best, eR);
         if (hL && rr.x < 0) { test_leaf(rr.x); hL = false; }
         if (hR && rr.y < 0) { if (eR <= t_best) test_leaf(rr.y); hR = false; }
-        if (hR && eR > t_best) hR = false;
+        hL = hL && eL <= t_best;
+        hR = hR && eR <= t_best;
         if (hL && hR) {
             if (eR < eL) { stk.push(sp, rr.x, eL); node = rr.y; }
             else { stk.push(sp, rr.y, eR); node = rr.x; }
@@ -556,9 +706,7 @@ __device__ int closest_hit(const SceneView& S, const Ray& ray, float tmin, float
     return best;
 }
 
-// Any hit in [tmin, tmax] (BVHNode::occluded, src/bvh.hpp:39-48). The box
-// test is order independent here (t_max is fixed), so the answer equals the
-// reference's.
+// Any hit of one ray in [tmin, tmax], traced to the end in one loop.
 template <int kShared, bool COUNT>
 __device__ bool any_hit(const SceneView& S, const Ray& ray, float tmin, float tmax,
                         TravStack<kShared>& stk, TravCount* cnt) {

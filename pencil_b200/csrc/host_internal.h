@@ -24,7 +24,7 @@ struct RenderCfg {
     uint32_t salt;
     int sample_offset;
     bool count;
-    int block;
+    int refill;
     int queue_capacity;
     int sort_key;
     bool profile;

@@ -35,6 +35,7 @@ namespace pgpu {
 constexpr int kWfShared = 16;
 constexpr int kWfBlock = 128;
 constexpr int kOctants = 8;
+constexpr int kDefaultRefill = 20;   // lanes still busy when a warp refetches
 
 // One render job of the path space.
 struct WfJob {
@@ -72,6 +73,8 @@ struct WfArgs {
     int* status;              // 1: shadow record overflow
     unsigned long long* counters;
     int sort_key;
+    int refill_below;         // extend/shadow: a warp refetches rays once at most
+                              // this many of its lanes are still traversing
 };
 
 __device__ __forceinline__ int find_job(const WfJob* jobs, int n, long long path) {
@@ -194,6 +197,10 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
 }
 
 // ---- extend -------------------------------------------------------------------
+// Persistent closest-hit traversal. A lane keeps its ray's traversal state
+// between node steps; when few lanes of the warp are still busy, the idle
+// lanes take new rays from the queue (one atomic per warp), so warps keep
+// traversing instead of waiting for their slowest ray.
 template <bool COUNT>
 __global__ void __launch_bounds__(kWfBlock)
 wf_extend(WfArgs A, int it) {
@@ -203,23 +210,47 @@ wf_extend(WfArgs A, int it) {
     stk.st = reinterpret_cast<float*>(smem + kWfShared * blockDim.x) + threadIdx.x;
     stk.stride = blockDim.x;
     RayCount rc = {};
-    QView qv = qview(A, it);
+    const QView qv = qview(A, it);
     unsigned int* cursor = A.work + it * 3 + 0;
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    ClosestTrav<kWfShared, COUNT> tr;
+    const SceneView* S = nullptr;
+    int slot = -1;
+    bool active = false;
+    bool exhausted = false;
     while (true) {
-        int base = fetch32(cursor);
-        if (base >= qv.total) break;
-        int e = base + (threadIdx.x & 31);
-        if (e < qv.total) {
-            int slot = qv.slot(e);
-            int jb = (int)A.st[slot].w;
-            const SceneView& S = A.views[A.jobs[jb].view];
-            float4 o = A.ray_o[slot], d = A.ray_d[slot];
-            Ray r{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)};
-            if (COUNT) rc.ext++;
-            float tb;
-            int bref;
-            int leaf = closest_hit<kWfShared, COUNT>(S, r, 1e-4f, 1e9f, tb, bref, stk, &rc.tc);
-            A.hit[slot] = make_float4(tb, __int_as_float(bref), __int_as_float(leaf), 0.0f);
+        unsigned act = __ballot_sync(0xffffffffu, active);
+        if (!exhausted && __popc(act) <= A.refill_below) {
+            const unsigned idle = ~act;
+            int base = 0;
+            if (lane == 0) base = (int)atomicAdd(cursor, (unsigned)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + __popc(idle) >= qv.total) exhausted = true;
+            if (!active) {
+                const int e = base + __popc(idle & below);
+                if (e < qv.total) {
+                    slot = qv.slot(e);
+                    S = &A.views[A.jobs[A.st[slot].w].view];
+                    const float4 o = A.ray_o[slot], d = A.ray_d[slot];
+                    if (COUNT) rc.ext++;
+                    if (tr.init(*S, Ray{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)}, 1e-4f, 1e9f, &rc.tc))
+                        A.hit[slot] = make_float4(tr.t_best, __int_as_float(tr.best_ref),
+                                                  __int_as_float(tr.best), 0.0f);
+                    else
+                        active = true;
+                }
+            }
+            act = __ballot_sync(0xffffffffu, active);
+        }
+        if (act == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        if (active && tr.step(*S, stk, &rc.tc)) {
+            A.hit[slot] = make_float4(tr.t_best, __int_as_float(tr.best_ref),
+                                      __int_as_float(tr.best), 0.0f);
+            active = false;
         }
     }
     flush_counts<COUNT>(A, rc, 1);
@@ -325,6 +356,10 @@ wf_shade(WfArgs A, int it) {
 }
 
 // ---- shadow -------------------------------------------------------------------
+// Persistent any-hit traversal of every slot's shadow records, with the same
+// lane refill as extend. A lane owns one slot: it resolves the slot's records
+// in the order shade made them, feeding each visibility into the same
+// NeeAccum as the megakernel, then applies the pending terms to L.
 template <bool COUNT>
 __global__ void __launch_bounds__(kWfBlock)
 wf_shadow(WfArgs A, int it) {
@@ -334,39 +369,80 @@ wf_shadow(WfArgs A, int it) {
     stk.st = reinterpret_cast<float*>(smem + kWfShared * blockDim.x) + threadIdx.x;
     stk.stride = blockDim.x;
     RayCount rc = {};
-    QView qv = qview(A, it);
+    const QView qv = qview(A, it);
     unsigned int* cursor = A.work + it * 3 + 2;
-    while (true) {
-        int base = fetch32(cursor);
-        if (base >= qv.total) break;
-        int e = base + (threadIdx.x & 31);
-        if (e < qv.total) {
-            int slot = qv.slot(e);
-            float4 pw = A.pw[slot];
-            int kind = __float_as_int(pw.w);
-            if (kind != 0) {
-                float4 pb = A.pb[slot], pt = A.pt[slot], L4 = A.L[slot];
-                const SceneView& S = A.views[A.jobs[A.st[slot].w].view];
-                NeeAccum acc;
-                if (kind == 1) acc.begin_pt();
-                else acc.begin_whitted(v3(pb.x, pb.y, pb.z));
-                V3 L = v3(L4.x, L4.y, L4.z);
-                int n = __float_as_int(pb.w);
-                for (int k = 0; k < n; ++k) {
-                    size_t idx = (size_t)k * A.Q + slot;
-                    float4 so = A.sh_o[idx], sd = A.sh_d[idx], sc = A.sh_c[idx];
-                    int bits = __float_as_int(sc.w);
-                    bool vis = true;
-                    if (bits & 1) {
-                        if (COUNT) rc.shadow++;
-                        Ray r{v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z)};
-                        vis = !any_hit<kWfShared, COUNT>(S, r, so.w, sd.w, stk, &rc.tc);
-                    }
-                    acc.add(L, v3(sc.x, sc.y, sc.z), bits >> 1, vis);
-                }
-                acc.finish(L, v3(pt.x, pt.y, pt.z), v3(pw.x, pw.y, pw.z), pt.w);
-                A.L[slot] = make_float4(L.x, L.y, L.z, 0.0f);
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    AnyTrav<kWfShared, COUNT> tr;
+    const SceneView* S = nullptr;
+    NeeAccum acc;
+    V3 L = v3(0, 0, 0), c = v3(0, 0, 0);
+    int slot = -1, k = 0, n = 0, group_end = 0;
+    bool active = false;
+    bool exhausted = false;
+
+    // Resolve records k, k+1, ... of this lane's slot until one needs a
+    // traversal (returns true) or all are done (pending terms applied).
+    auto advance = [&]() -> bool {
+        while (k < n) {
+            const size_t idx = (size_t)k * A.Q + slot;
+            const float4 sc = A.sh_c[idx];
+            const int bits = __float_as_int(sc.w);
+            c = v3(sc.x, sc.y, sc.z);
+            group_end = bits >> 1;
+            if (bits & 1) {
+                const float4 so = A.sh_o[idx], sd = A.sh_d[idx];
+                if (COUNT) rc.shadow++;
+                if (!tr.init(*S, Ray{v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z)}, so.w, sd.w,
+                             &rc.tc))
+                    return true;
+                acc.add(L, c, group_end, !tr.hit);
+            } else {
+                acc.add(L, c, group_end, true);
             }
+            ++k;
+        }
+        const float4 pt = A.pt[slot], pw = A.pw[slot];
+        acc.finish(L, v3(pt.x, pt.y, pt.z), v3(pw.x, pw.y, pw.z), pt.w);
+        A.L[slot] = make_float4(L.x, L.y, L.z, 0.0f);
+        return false;
+    };
+
+    while (true) {
+        unsigned act = __ballot_sync(0xffffffffu, active);
+        if (!exhausted && __popc(act) <= A.refill_below) {
+            const unsigned idle = ~act;
+            int base = 0;
+            if (lane == 0) base = (int)atomicAdd(cursor, (unsigned)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + __popc(idle) >= qv.total) exhausted = true;
+            if (!active) {
+                const int e = base + __popc(idle & below);
+                if (e < qv.total) {
+                    slot = qv.slot(e);
+                    const int kind = __float_as_int(A.pw[slot].w);
+                    if (kind != 0) {
+                        S = &A.views[A.jobs[A.st[slot].w].view];
+                        const float4 pb = A.pb[slot], L4 = A.L[slot];
+                        if (kind == 1) acc.begin_pt();
+                        else acc.begin_whitted(v3(pb.x, pb.y, pb.z));
+                        L = v3(L4.x, L4.y, L4.z);
+                        n = __float_as_int(pb.w);
+                        k = 0;
+                        active = advance();
+                    }
+                }
+            }
+            act = __ballot_sync(0xffffffffu, active);
+        }
+        if (act == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        if (active && tr.step(*S, stk, &rc.tc)) {
+            acc.add(L, c, group_end, !tr.hit);
+            ++k;
+            active = advance();
         }
     }
     flush_counts<COUNT>(A, rc, 2);
@@ -640,7 +716,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     int iters = 0, maxS = 1, max_spp = 1;
     long long total_paths = 0;
     bool count = false;
-    int qcap = 0, sort_key = 0;
+    int qcap = 0, sort_key = 0, refill = 0;
     for (int k = 0; k < n; ++k) {
         const RenderCfg& c = cfgs[k];
         WfJob& J = jobs[k];
@@ -660,9 +736,10 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
         count = count || c.count;
         if (c.queue_capacity > 0) qcap = c.queue_capacity;
         sort_key = c.sort_key;
+        if (c.refill > 0) refill = c.refill;
     }
     total_paths = path_off;
-    long long Q = qcap > 0 ? qcap : (1LL << 21);
+    long long Q = qcap > 0 ? qcap : (1LL << 22);
     Q = std::max<long long>(Q, max_spp);
     Q = std::min<long long>(Q, total_paths);
     Q = std::max<long long>(Q, 1);
@@ -671,6 +748,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     W.args.n_jobs = n;
     W.args.counters = counters;
     W.args.sort_key = sort_key;
+    W.args.refill_below = refill > 0 ? refill : kDefaultRefill;
     W.args.maxS = maxS;
     if ((e = cudaMemcpyAsync(W.d_views, views.data(), views.size() * sizeof(SceneView),
                              cudaMemcpyHostToDevice, st)) != cudaSuccess)
@@ -686,6 +764,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     mix((unsigned long long)Q);
     mix((unsigned long long)maxS);
     mix((unsigned long long)sort_key);
+    mix((unsigned long long)W.args.refill_below);
     mix((unsigned long long)count);
     for (const auto& J : jobs) {
         mix((unsigned long long)J.P.W); mix((unsigned long long)J.P.H);
@@ -857,6 +936,7 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
     A.jobs = d_job;
     A.counters = nullptr;
     A.sort_key = 0;
+    A.refill_below = kDefaultRefill;
     WfJob J;
     J.P = PathParams{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias,
                      c.salt, c.sample_offset};

@@ -45,6 +45,7 @@ class RenderSettings:
     profile_kernels: bool = False
     queue_capacity: int = 0
     sort_key: int = 0
+    refill_below: int = 0
 
     def params(self) -> A.RenderParams:
         p = A.RenderParams()
@@ -61,6 +62,7 @@ class RenderSettings:
                    (0 if self.use_graph else A.FLAG_NO_GRAPH) |
                    (A.FLAG_PROFILE_KERNELS if self.profile_kernels else 0))
         p.queue_capacity, p.sort_key = self.queue_capacity, self.sort_key
+        p.refill_below = self.refill_below
         return p
 
 
