@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the adjoint, batch and image-quality measurements")
     ap.add_argument("--profile-case", choices=["wavefront", "megakernel"], default=None,
                     help="render the workload once, kernels launched one by one (for ncu)")
     ap.add_argument("--profile-scale", type=int, default=1,
@@ -341,6 +343,10 @@ def run_ours(args) -> None:
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": sec * 1e3,
                "ms_upload_render_free": [round(float(x), 3) for x in ph]}
 
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        extras = measure_extras(ctx, sid, st, img, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -376,11 +382,103 @@ def run_ours(args) -> None:
             "clocks": clk,
             "gpu_launches": launches_per_frame * args.steps,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     ctx.free(sid)
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def _event_ms(stream, fn, reps: int) -> float:
+    import torch
+    fn()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def measure_extras(ctx, sid, st, img, stream) -> dict:
+    """Outside the timed region: image quality against a 4096-spp render of
+    the bench frame, the adjoint of the box configuration, and the batch of
+    256 uneven scenes."""
+    import dataclasses
+
+    import torch
+    from pencil_b200 import _abi as A
+    from pencil_b200 import workloads as W
+    out = {}
+    # quality: relative RMSE of the 16-spp frame against 4096 spp (256 frames
+    # of 16 spp with distinct sample offsets, averaged on the device)
+    ref = torch.zeros_like(img)
+    q = dataclasses.replace(st, engine=A.ENGINE_WAVEFRONT)
+    frames = 256
+    for k in range(frames):
+        q.sample_offset = (k + 1000) * st.samples * st.samples
+        ctx.render_device(sid, q, img.data_ptr())
+        ref += img
+    ref /= frames
+    q.sample_offset = 0
+    ctx.render_device(sid, q, img.data_ptr())
+    rel_rmse = float(torch.sqrt(((img - ref) ** 2).mean()) / ref.mean())
+    spp = st.samples ** 2
+    out["quality"] = {"rel_rmse_vs_4096spp": rel_rmse, "spp": spp,
+                      "spp_for_1pct_rmse": int(np.ceil(spp * (rel_rmse / 0.01) ** 2)),
+                      "note": "wavefront and megakernel images are bit-identical, so their RMSE "
+                              "is equal at every spp"}
+    # adjoint of the box configuration: 1,000 spheres, 512x512, 16 spp, depth 6
+    wa, _, _ = W.adjoint_box()
+    sa = ctx.upload(wa.scene)
+    ast = wa.settings
+    buf = torch.empty((ast.height, ast.width, 3), dtype=torch.float32, device="cuda")
+    fwd_ms = _event_ms(stream, lambda: ctx.render_device(sa, ast, buf.data_ptr()), 5)
+    dl = np.random.default_rng(0).normal(size=(ast.height, ast.width, 3)).astype(np.float32)
+    from pencil_b200.renderer import RenderStats
+    adj = []
+    for _ in range(4):
+        s_ = RenderStats()
+        ctx.adjoint(sa, ast, dl, wa.scene.n_materials, len(wa.scene.lights), stats=s_)
+        adj.append(s_.device_ms)
+    adj_ms = float(np.median(adj[1:]))
+    out["adjoint"] = {"workload": "adjoint_box_1000spheres_512x512_16spp_depth6",
+                      "ms_per_grad": adj_ms, "forward_ms": fwd_ms,
+                      "grad_over_forward": adj_ms / fwd_ms,
+                      "parameters": 3 * wa.scene.n_materials + 3 * len(wa.scene.lights)}
+    ctx.free(sa)
+    # batch: 256 uneven scenes in one launch sequence against one at a time
+    jobs = W.sphere_batch()
+    sids = [ctx.upload(j.scene) for j in jobs]
+    sts = [j.settings for j in jobs]
+    outs = [torch.empty((x.height, x.width, 3), dtype=torch.float32, device="cuda") for x in sts]
+    ptrs = [o.data_ptr() for o in outs]
+    paths = sum(x.width * x.height * x.samples ** 2 for x in sts)
+    for x in sts:
+        x.queue_capacity, x.refill_below = 1 << 24, 16
+    batch_ms = _event_ms(stream, lambda: ctx.render_batch(sids, sts, device_ptrs=ptrs), 2)
+
+    def one_by_one(engine):
+        for sid_, x, p_ in zip(sids, sts, ptrs):
+            x.engine = engine
+            ctx.render_device(sid_, x, p_)
+    seq_ms = _event_ms(stream, lambda: one_by_one(A.ENGINE_WAVEFRONT), 1)
+    mk_ms = _event_ms(stream, lambda: one_by_one(A.ENGINE_MEGAKERNEL), 1)
+    for x in sts:
+        x.engine = A.ENGINE_WAVEFRONT
+    out["batch"] = {"workload": "256 random-sphere scenes, 10-50,000 spheres, 128/256/512 "
+                                "squared, 1/4/16/64 spp, depth 8",
+                    "paths": paths, "batched_mpaths_s": paths / batch_ms / 1e3,
+                    "one_by_one_wavefront_mpaths_s": paths / seq_ms / 1e3,
+                    "one_by_one_megakernel_mpaths_s": paths / mk_ms / 1e3,
+                    "batched_ms": batch_ms, "one_by_one_wavefront_ms": seq_ms,
+                    "one_by_one_megakernel_ms": mk_ms}
+    for s_ in sids:
+        ctx.free(s_)
+    return out
 
 
 class _Null:

@@ -1012,6 +1012,344 @@ int32_t orc_render_split(const orc_scene* s, const pgpu_render_params* p, float*
     return 0;
 }
 
+/* ---- FP64 adjoint of the production estimator ---------------------------------
+ * Test-only restatement of pencil_b200/csrc/adjoint.cu: each path is replayed
+ * with exactly the float32 geometry and decisions of the production
+ * estimator (the float throughput drives Russian roulette, as on the GPU);
+ * the tape, the backward sweep and every gradient sum are kept in double. */
+typedef struct { double x, y, z; } dv3;
+static inline dv3 dvk(double x, double y, double z) { dv3 r = {x, y, z}; return r; }
+static inline dv3 dvf(v3 a) { return dvk(a.x, a.y, a.z); }
+static inline dv3 dvadd(dv3 a, dv3 b) { return dvk(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline dv3 dvmul(dv3 a, dv3 b) { return dvk(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline dv3 dvs(dv3 a, double s) { return dvk(a.x * s, a.y * s, a.z * s); }
+
+#define ADJ_MAX_TAPE 16
+
+typedef struct {
+    int mat;
+    dv3 T, B, g, A;
+} tape_t;
+
+typedef struct {
+    const orc_scene* s;
+    const pgpu_render_params* p;
+    const char* area_emitter;
+    const float* quad_area;
+    int has_quad;
+    double* d_albedo;   /* per thread accumulators (3 per material) */
+    double* d_emission;
+    double* d_light;
+    trav_t tv;
+} adj_ctx;
+
+/* Replay one path; returns its radiance (double) and adds to the gradients. */
+static dv3 adj_path(adj_ctx* a, ray_t r, rng_t* rng, dv3 w) {
+    const orc_scene* s = a->s;
+    const pgpu_render_params* P = a->p;
+    tape_t tape[ADJ_MAX_TAPE];
+    int nt = 0;
+    v3 Tf = mk(1, 1, 1);               /* float throughput: drives decisions */
+    dv3 T = dvk(1, 1, 1), L = dvk(0, 0, 0);
+    int depth = P->depth;
+    unsigned flags = P->mode == PGPU_MODE_WHITTED ? SPL_WHITTED : 0u;
+    int alive = depth > 0;
+    while (alive && nt < ADJ_MAX_TAPE) {
+        tape_t* tv = &tape[nt++];
+        tv->T = T;
+        tv->B = dvk(0, 0, 0);
+        tv->g = dvk(0, 0, 0);
+        hitrec h;
+        if (!scene_hit(&a->tv, r, 1e-4f, 1e9f, &h)) {
+            tv->mat = -1;
+            tv->A = dvf(ld3(s->background));
+            L = dvadd(L, dvmul(T, tv->A));
+            break;
+        }
+        const pgpu_material* m = &s->materials[h.mat];
+        const v3 albedo = ld3(m->albedo);
+        const dv3 ad = dvf(albedo);
+        const int metal = m->kind == PGPU_MAT_METAL && m->reflectivity > 0.0f;
+        const int glass = m->kind == PGPU_MAT_DIELECTRIC;
+        const v3 sorg = add(h.p, mulf(h.n, P->shadow_bias));
+        tv->mat = h.mat;
+        dv3 e = dvk(0, 0, 0);
+        int dielectric = 0;
+        alive = 0;
+        if (!(flags & SPL_WHITTED)) {
+            const int diffuse = !metal && !glass;
+            if (!glass && !((flags & SPL_SKIP_AREA) && a->area_emitter[h.mat])) {
+                e = dvf(ld3(m->emission));
+                double* g = a->d_emission + 3 * h.mat;
+                dv3 c = dvmul(w, T);
+                g[0] += c.x; g[1] += c.y; g[2] += c.z;
+            }
+            for (int li = 0; li < s->n_lights; ++li) {
+                const pgpu_light* l = &s->lights[li];
+                if (l->kind == PGPU_LIGHT_QUAD) continue;
+                v3 Ld; float dist;
+                light_dir(l, h.p, rng, &Ld, &dist);
+                float ndotl = clampf(dot(h.n, Ld), 0.0f, 1.0f);
+                ray_t sr = {sorg, Ld};
+                int vis = l->is_emissive || !scene_occ(&a->tv, sr, P->shadow_bias, dist - P->shadow_bias);
+                if (!vis) continue;
+                tv->B = dvadd(tv->B, dvs(dvf(ld3(l->intensity)), ndotl));
+                dv3 c = dvs(dvmul(dvmul(w, T), ad), ndotl);
+                a->d_light[3 * li] += c.x; a->d_light[3 * li + 1] += c.y; a->d_light[3 * li + 2] += c.z;
+            }
+            if (a->has_quad && diffuse && depth - 1 > 0) {
+                for (int li = 0; li < s->n_lights; ++li) {
+                    const pgpu_light* l = &s->lights[li];
+                    if (l->kind != PGPU_LIGHT_QUAD) continue;
+                    v3 Ld; float tmax, wq;
+                    if (!quad_sample(l, a->quad_area[li], h.p, h.n, sorg, P->shadow_bias, rng,
+                                     &Ld, &tmax, &wq)) continue;
+                    ray_t sr = {sorg, Ld};
+                    if (scene_occ(&a->tv, sr, P->shadow_bias, tmax)) continue;
+                    tv->B = dvadd(tv->B, dvs(dvf(ld3(l->intensity)), wq));
+                    dv3 c = dvs(dvmul(dvmul(w, T), ad), wq);
+                    a->d_light[3 * li] += c.x; a->d_light[3 * li + 1] += c.y; a->d_light[3 * li + 2] += c.z;
+                }
+            }
+            tv->B = dvadd(tv->B, dvf(ld3(s->ambient)));
+            tv->A = dvadd(e, dvmul(ad, tv->B));
+            L = dvadd(L, dvmul(T, tv->A));
+            double inv_p = 1.0;
+            if (P->depth - depth > 3) {
+                float pr = fmaxf(Tf.x, fmaxf(Tf.y, Tf.z));
+                if (rng_unit(rng) > pr) break;
+                Tf = divf(Tf, pr);
+                inv_p = 1.0 / (double)pr;
+                T = dvs(T, inv_p);
+            }
+            if (!glass) {
+                v3 nd;
+                if (metal) {
+                    v3 refl = nrm(reflect(nrm(r.d), h.n));
+                    v3 upv = (fabsf(refl.y) < 0.9f) ? mk(0, 1, 0) : mk(1, 0, 0);
+                    v3 t1 = nrm(cross(refl, upv));
+                    v3 t2 = nrm(cross(refl, t1));
+                    float r1 = rng_unit(rng) * 0.1f;
+                    float r2 = rng_unit(rng) * 6.28f;
+                    nd = nrm(add(add(refl, mulf(t1, r1 * cosf(r2))), mulf(t2, r1 * sinf(r2))));
+                    Tf = mulf(mulv(Tf, albedo), m->reflectivity);
+                    T = dvs(dvmul(T, ad), m->reflectivity);
+                    tv->g = dvs(dvk(inv_p, inv_p, inv_p), m->reflectivity);
+                } else {
+                    float r1 = rng_unit(rng) * 6.2831853f;
+                    float r2 = rng_unit(rng);
+                    float r2s = sqrtf(r2);
+                    v3 N = h.n;
+                    v3 upv = (fabsf(N.y) < 0.9f) ? mk(0, 1, 0) : mk(1, 0, 0);
+                    v3 Tn = nrm(cross(upv, N));
+                    v3 B = nrm(cross(N, Tn));
+                    nd = nrm(add(add(mulf(mulf(Tn, cosf(r1)), r2s), mulf(mulf(B, sinf(r1)), r2s)),
+                                 mulf(N, sqrtf(1.0f - r2))));
+                    Tf = mulv(Tf, albedo);
+                    T = dvmul(T, ad);
+                    tv->g = dvk(inv_p, inv_p, inv_p);
+                }
+                flags = (diffuse && a->has_quad) ? SPL_SKIP_AREA : 0u;
+                r.o = sorg;
+                r.d = nd;
+                depth--;
+                alive = depth > 0;
+                if (!alive) tv->g = dvk(0, 0, 0);
+                continue;
+            }
+            tv->g = dvk(inv_p, inv_p, inv_p);
+            dielectric = 1;
+        } else {
+            dv3 sum_a = dvk(0, 0, 0), sum_e = dvk(0, 0, 0);
+            double sc = 1.0;
+            if (!glass) {
+                sum_e = dvf(ld3(m->emission));
+                sc = metal ? (double)(1.0f - m->reflectivity) : 1.0;
+            }
+            for (int li = 0; li < s->n_lights; ++li) {
+                const pgpu_light* l = &s->lights[li];
+                if (l->kind == PGPU_LIGHT_QUAD) continue;
+                int ns = (l->radius > 0.0f) ? P->soft_shadow_samples : 1;
+                dv3 ca = dvk(0, 0, 0), ce = dvk(0, 0, 0);
+                for (int k = 0; k < ns; ++k) {
+                    v3 Ld; float dist;
+                    light_dir(l, h.p, rng, &Ld, &dist);
+                    if (glass) continue;
+                    float ndotl = clampf(dot(h.n, Ld), 0.0f, 1.0f);
+                    v3 phong = mk(0, 0, 0);
+                    if (m->specular > 0.0f && ndotl > 0.0f) {
+                        v3 V = neg(nrm(r.d));
+                        v3 H = nrm(add(Ld, V));
+                        float ndoth = clampf(dot(h.n, H), 0.0f, 1.0f);
+                        float spec = powf(ndoth, m->shininess);
+                        phong = mulf(ld3(m->specular_color), spec * m->specular);
+                    }
+                    ray_t sr = {sorg, Ld};
+                    if (!l->is_emissive && scene_occ(&a->tv, sr, P->shadow_bias, dist - P->shadow_bias)) continue;
+                    ca = dvadd(ca, dvs(dvf(ld3(l->intensity)), ndotl));
+                    ce = dvadd(ce, dvmul(dvf(ld3(l->intensity)), dvf(phong)));
+                    dv3 c = dvs(dvmul(dvmul(w, T), dvadd(dvs(ad, ndotl), dvf(phong))), sc / ns);
+                    a->d_light[3 * li] += c.x; a->d_light[3 * li + 1] += c.y; a->d_light[3 * li + 2] += c.z;
+                }
+                sum_a = dvadd(sum_a, dvs(ca, 1.0 / ns));
+                sum_e = dvadd(sum_e, dvs(ce, 1.0 / ns));
+            }
+            if (!glass) {
+                double* g = a->d_emission + 3 * h.mat;
+                dv3 c = dvs(dvmul(w, T), sc);
+                g[0] += c.x; g[1] += c.y; g[2] += c.z;
+                tv->B = dvs(dvadd(sum_a, dvf(ld3(s->ambient))), sc);
+                tv->A = dvadd(dvs(sum_e, sc), dvmul(ad, tv->B));
+                L = dvadd(L, dvmul(T, tv->A));
+                if (metal) {
+                    Tf = mulf(mulv(Tf, albedo), m->reflectivity);
+                    T = dvs(dvmul(T, ad), m->reflectivity);
+                    tv->g = dvk(m->reflectivity, m->reflectivity, m->reflectivity);
+                    r.o = sorg;
+                    r.d = nrm(reflect(nrm(r.d), h.n));
+                    depth--;
+                    alive = depth > 0;
+                    if (!alive) tv->g = dvk(0, 0, 0);
+                }
+                continue;
+            }
+            tv->A = dvk(0, 0, 0);
+            tv->g = dvk(1, 1, 1);
+            dielectric = 1;
+        }
+        if (dielectric) {
+            float safe = fmaxf(m->ior, 0.01f);
+            float eta = h.front ? (1.0f / safe) : safe;
+            v3 ndr = nrm(r.d);
+            float cos_i = fabsf(dot(ndr, h.n));
+            float sin_t2 = eta * eta * (1.0f - cos_i * cos_i);
+            ray_t refl = {add(h.p, mulf(h.n, P->shadow_bias)), nrm(reflect(ndr, h.n))};
+            int tir = sin_t2 > 1.0f;
+            float kr = 1.0f;
+            ray_t refr = refl;
+            if (!tir) {
+                float cos_t = sqrtf(1.0f - sin_t2);
+                refr.o = sub(h.p, mulf(h.n, P->shadow_bias));
+                refr.d = nrm(add(mulf(ndr, eta), mulf(h.n, eta * cos_i - cos_t)));
+                kr = schlick(h.front ? cos_i : cos_t, eta);
+            }
+            if (tir || rng_unit(rng) < kr) r = refl;
+            else r = refr;
+            Tf = mulv(Tf, albedo);
+            T = dvmul(T, ad);
+            depth--;
+            flags = SPL_WHITTED;
+            alive = depth > 0;
+            if (!alive) tv->g = dvk(0, 0, 0);
+        }
+    }
+    /* backward sweep */
+    dv3 R = dvk(0, 0, 0);
+    for (int k = nt - 1; k >= 0; --k) {
+        tape_t* tv = &tape[k];
+        if (tv->mat >= 0) {
+            dv3 ad = dvf(ld3(s->materials[tv->mat].albedo));
+            dv3 c = dvmul(dvmul(w, tv->T), dvadd(tv->B, dvmul(tv->g, R)));
+            double* g = a->d_albedo + 3 * tv->mat;
+            g[0] += c.x; g[1] += c.y; g[2] += c.z;
+            R = dvadd(tv->A, dvmul(dvmul(ad, tv->g), R));
+        } else {
+            R = tv->A;
+        }
+    }
+    return L;
+}
+
+typedef struct {
+    adj_ctx a;
+    const float* dl;
+    double* img;        /* per-pixel radiance sums (double) */
+    int row0, stride;
+} ajob_t;
+
+static void* adj_thread(void* arg) {
+    ajob_t* jb = (ajob_t*)arg;
+    adj_ctx* a = &jb->a;
+    const pgpu_render_params* p = a->p;
+    const int W = p->width, H = p->height, n = p->samples, spp = n * n;
+    for (int j = jb->row0; j < H; j += jb->stride) {
+        for (int i = 0; i < W; ++i) {
+            size_t o = ((size_t)j * W + i) * 3;
+            dv3 w = dvk((double)jb->dl[o] / spp, (double)jb->dl[o + 1] / spp, (double)jb->dl[o + 2] / spp);
+            dv3 acc = dvk(0, 0, 0);
+            for (int smp = 0; smp < spp; ++smp) {
+                rng_t rng = {orc_path_seed(i, j, smp + p->sample_offset, p->seed)};
+                float u = (i + ((smp % n) + 0.5f) / n) / (float)W;
+                float v = 1.0f - (j + ((smp / n) + 0.5f) / n) / (float)H;
+                u += rng_sym(&rng) * (0.5f / (W * n));
+                v += rng_sym(&rng) * (0.5f / (H * n));
+                acc = dvadd(acc, adj_path(a, camera_ray(a->s, u, v), &rng, w));
+            }
+            if (jb->img) {
+                jb->img[o] = acc.x / spp; jb->img[o + 1] = acc.y / spp; jb->img[o + 2] = acc.z / spp;
+            }
+        }
+    }
+    return NULL;
+}
+
+int32_t orc_adjoint(const orc_scene* s, const pgpu_render_params* p, const float* dl,
+                    double* d_albedo, double* d_emission, double* d_light, double* out_img,
+                    int32_t n_threads) {
+    if (!s || !p || !dl || !d_albedo || !d_emission) return -1;
+    if (p->depth > ADJ_MAX_TAPE) return -1;
+    const int nm = s->n_materials, nl = s->n_lights;
+    char* area_emitter = (char*)calloc((size_t)(nm > 0 ? nm : 1), 1);
+    float* quad_area = (float*)calloc((size_t)(nl > 0 ? nl : 1), sizeof(float));
+    int has_quad = 0;
+    for (int k = 0; k < nl; ++k) {
+        const pgpu_light* l = &s->lights[k];
+        if (l->kind != PGPU_LIGHT_QUAD) continue;
+        v3 cr = cross(ld3(l->edge_u), ld3(l->edge_v));
+        quad_area[k] = sqrtf(cr.x * cr.x + cr.y * cr.y + cr.z * cr.z);
+        if (l->material >= 0 && l->material < nm) area_emitter[l->material] = 1;
+        has_quad = 1;
+    }
+    if (n_threads < 1) n_threads = 1;
+    if (n_threads > p->height) n_threads = p->height;
+    ajob_t* jobs = (ajob_t*)calloc((size_t)n_threads, sizeof(ajob_t));
+    pthread_t* th = (pthread_t*)calloc((size_t)n_threads, sizeof(pthread_t));
+    char* live = (char*)calloc((size_t)n_threads, 1);
+    for (int k = 0; k < n_threads; ++k) {
+        ajob_t* jb = &jobs[k];
+        jb->a.s = s; jb->a.p = p; jb->a.area_emitter = area_emitter; jb->a.quad_area = quad_area;
+        jb->a.has_quad = has_quad;
+        jb->a.d_albedo = (double*)calloc((size_t)nm * 3 + 1, sizeof(double));
+        jb->a.d_emission = (double*)calloc((size_t)nm * 3 + 1, sizeof(double));
+        jb->a.d_light = (double*)calloc((size_t)nl * 3 + 1, sizeof(double));
+        jb->a.tv.s = s; jb->a.tv.cnt = NULL;
+        jb->dl = dl; jb->img = out_img; jb->row0 = k; jb->stride = n_threads;
+    }
+    for (int k = 1; k < n_threads; ++k)
+        live[k] = pthread_create(&th[k], NULL, adj_thread, &jobs[k]) == 0;
+    adj_thread(&jobs[0]);
+    for (int k = 1; k < n_threads; ++k) {
+        if (live[k]) pthread_join(th[k], NULL);
+        else adj_thread(&jobs[k]);
+    }
+    for (int q = 0; q < nm * 3; ++q) {
+        double sa = 0, se = 0;
+        for (int k = 0; k < n_threads; ++k) { sa += jobs[k].a.d_albedo[q]; se += jobs[k].a.d_emission[q]; }
+        d_albedo[q] = sa; d_emission[q] = se;
+    }
+    if (d_light)
+        for (int q = 0; q < nl * 3; ++q) {
+            double sl = 0;
+            for (int k = 0; k < n_threads; ++k) sl += jobs[k].a.d_light[q];
+            d_light[q] = sl;
+        }
+    for (int k = 0; k < n_threads; ++k) {
+        free(jobs[k].a.d_albedo); free(jobs[k].a.d_emission); free(jobs[k].a.d_light);
+    }
+    free(jobs); free(th); free(live); free(area_emitter); free(quad_area);
+    return 0;
+}
+
 /* ---- ray queries ---------------------------------------------------------- */
 void orc_trace_rays(const orc_scene* s, const float* rays, int32_t n, int32_t* prim_id,
                     float* t, uint64_t* counters) {

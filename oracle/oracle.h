@@ -72,6 +72,15 @@ int32_t orc_render_split(const orc_scene* s, const pgpu_render_params* p,
                          float* out_rgb, float* out_m2, int32_t n_threads,
                          uint64_t* counters);
 
+/* FP64 adjoint of the production estimator (test-only): replays each path
+ * with the float32 geometry and decisions of orc_render_split and
+ * accumulates, in double, dLoss/d(albedo), dLoss/d(emission) (3 per
+ * material) and dLoss/d(intensity) (3 per light) for the pixel weights
+ * dl (= dLoss/dimage, W*H*3). out_img (optional) gets the replayed image. */
+int32_t orc_adjoint(const orc_scene* s, const pgpu_render_params* p, const float* dl,
+                    double* d_albedo, double* d_emission, double* d_light,
+                    double* out_img, int32_t n_threads);
+
 /* Closest hit in the reference's traversal order (left subtree first,
  * t_max clipped by the left result), t_min 1e-4, t_max 1e9. */
 void orc_trace_rays(const orc_scene* s, const float* rays, int32_t n,

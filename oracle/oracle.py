@@ -57,6 +57,9 @@ def load():
     lib.orc_render.restype = C.c_int32
     lib.orc_render_split.argtypes = lib.orc_render.argtypes
     lib.orc_render_split.restype = C.c_int32
+    lib.orc_adjoint.argtypes = [C.POINTER(OrcScene), C.POINTER(A.RenderParams), C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
+    lib.orc_adjoint.restype = C.c_int32
     lib.orc_trace_rays.argtypes = [C.POINTER(OrcScene), C.c_void_p, C.c_int32, C.c_void_p,
                                    C.c_void_p, C.c_void_p]
     lib.orc_primary_hits.argtypes = [C.POINTER(OrcScene), C.c_void_p, C.c_int32, C.c_void_p,
@@ -120,6 +123,22 @@ class Oracle:
         if rc != 0:
             raise ValueError("orc_render_split rejected its arguments")
         return out, m2, cnt
+
+    def adjoint(self, settings, dl: np.ndarray, threads: int | None = None):
+        """FP64 CPU adjoint of the production estimator: returns
+        (d_albedo (n_mat,3), d_emission (n_mat,3), d_light (n_light,3),
+        replayed image (H,W,3) float64)."""
+        p = settings.params()
+        dl = np.ascontiguousarray(dl, np.float32)
+        nm, nl = len(self.mats), len(self.lights)
+        da, de = np.zeros((nm, 3)), np.zeros((nm, 3))
+        dli = np.zeros((max(nl, 1), 3))
+        img = np.zeros((settings.height, settings.width, 3))
+        rc = self.lib.orc_adjoint(C.byref(self.s), C.byref(p), A.ptr(dl), A.ptr(da), A.ptr(de),
+                                  A.ptr(dli), A.ptr(img), threads or os.cpu_count() or 1)
+        if rc != 0:
+            raise ValueError("orc_adjoint rejected its arguments")
+        return da, de, dli[:nl], img
 
     def trace_rays(self, rays: np.ndarray, counters: bool = False):
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)

@@ -20,7 +20,7 @@ BUILD = HERE / "_build"
 LIB = HERE / "libpencil_gpu.so"
 INCLUDE = HERE.parent / "include"
 
-CU_SOURCES = ["api.cu", "megakernel.cu", "wavefront.cu", "queries.cu"]
+CU_SOURCES = ["api.cu", "megakernel.cu", "wavefront.cu", "queries.cu", "adjoint.cu"]
 CXX_SOURCES = ["bvh_build.cpp"]
 HEADERS = ["device_common.cuh", "path.cuh", "scene_layout.h", "host_internal.h"]
 

@@ -38,6 +38,11 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
                                     float* m2, cudaStream_t st, int* status_host, int* launches,
                                     const char** why);
 size_t static_scratch_bytes();
+cudaError_t launch_adjoint(const SceneView& S, const RenderCfg& c, const float* dl,
+                           double* d_albedo, double* d_emission, double* d_light, float* out,
+                           unsigned long long* counters, cudaStream_t st);
+int adjoint_max_depth();
+int adjoint_max_lights();
 
 constexpr int kMaxDepth = 64;          // traversal stack bound (kMaxStack)
 constexpr int kMaxTreeFrames = 32;     // Whitted recursion bound of the two-branch mode
@@ -119,6 +124,8 @@ struct pgpu_ctx {
     int* h_status = nullptr;          // pinned
     unsigned char* h_stage = nullptr; // pinned staging of scene uploads
     size_t stage_cap = 0;
+    unsigned char* d_adj = nullptr;   // adjoint inputs and gradient sums
+    size_t adj_cap = 0;
 };
 
 namespace {
@@ -265,6 +272,7 @@ void pgpu_destroy(pgpu_ctx* c) {
     cudaFree(c->d_m2);
     cudaFree(c->d_cnt);
     cudaFree(c->d_query);
+    cudaFree(c->d_adj);
     wavefront_delete(c->wf);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -828,9 +836,65 @@ int32_t pgpu_render_batch(pgpu_ctx* c, int32_t n_jobs, const int32_t* ids,
 int32_t pgpu_adjoint(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, const float* dl,
                      double* d_albedo, double* d_emission, double* d_light, float* out_rgb,
                      pgpu_stats* stats) {
-    (void)id; (void)p; (void)dl; (void)d_albedo; (void)d_emission; (void)d_light; (void)out_rgb;
-    (void)stats;
-    return fail(c, PGPU_ERR_UNSUPPORTED, "adjoint not built yet");
+    auto t0 = std::chrono::steady_clock::now();
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    DeviceScene* ds = find_scene(c, id);
+    if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
+    if (!dl || !d_albedo || !d_emission || (!d_light && !ds->lights.empty()))
+        return fail(c, PGPU_ERR_INVALID_ARG, "null adjoint buffer");
+    RenderCfg cfg;
+    int rc = make_cfg(c, ds, p, cfg);
+    if (rc) return rc;
+    if (cfg.rng != PGPU_RNG_COUNTER || cfg.glass != PGPU_GLASS_FRESNEL_SPLIT)
+        return fail(c, PGPU_ERR_UNSUPPORTED, "the adjoint replays the counter-RNG, Fresnel-split estimator");
+    if (cfg.depth > adjoint_max_depth())
+        return fail(c, PGPU_ERR_UNSUPPORTED, "adjoint depth is limited to %d", adjoint_max_depth());
+    if ((int)ds->lights.size() > adjoint_max_lights())
+        return fail(c, PGPU_ERR_UNSUPPORTED, "adjoint supports at most %d lights", adjoint_max_lights());
+    PGPU_CUDA(c, cudaSetDevice(c->device));
+    const size_t n3 = (size_t)cfg.W * cfg.H * 3;
+    const size_t nm = ds->mats.size(), nl = ds->lights.size();
+    const size_t grad_b = (2 * nm + nl) * 3 * sizeof(double);
+    const size_t need = align256(n3 * 4) + align256(n3 * 4) + align256(grad_b);
+    if ((rc = ensure(c, c->d_adj, c->adj_cap, need))) return rc;
+    float* d_dl = reinterpret_cast<float*>(c->d_adj);
+    float* d_img = reinterpret_cast<float*>(c->d_adj + align256(n3 * 4));
+    double* d_g = reinterpret_cast<double*>(c->d_adj + 2 * align256(n3 * 4));
+    PGPU_CUDA(c, cudaMemcpyAsync(d_dl, dl, n3 * 4, cudaMemcpyHostToDevice, c->stream));
+    PGPU_CUDA(c, cudaMemsetAsync(d_g, 0, grad_b, c->stream));
+    if (cfg.count)
+        PGPU_CUDA(c, cudaMemsetAsync(c->d_cnt, 0, CNT_N * sizeof(unsigned long long), c->stream));
+    PGPU_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    cudaError_t e = launch_adjoint(ds->view, cfg, d_dl, d_g, d_g + 3 * nm, d_g + 6 * nm,
+                                   out_rgb ? d_img : nullptr, c->d_cnt, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "adjoint launch");
+    PGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    PGPU_CUDA(c, cudaMemcpyAsync(d_albedo, d_g, nm * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PGPU_CUDA(c, cudaMemcpyAsync(d_emission, d_g + 3 * nm, nm * 3 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->stream));
+    if (nl)
+        PGPU_CUDA(c, cudaMemcpyAsync(d_light, d_g + 6 * nm, nl * 3 * sizeof(double),
+                                     cudaMemcpyDeviceToHost, c->stream));
+    if (out_rgb)
+        PGPU_CUDA(c, cudaMemcpyAsync(out_rgb, d_img, n3 * 4, cudaMemcpyDeviceToHost, c->stream));
+    unsigned long long cnt[CNT_N] = {0};
+    if (cfg.count)
+        PGPU_CUDA(c, cudaMemcpyAsync(cnt, c->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+    PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        stats->device_ms = ms;
+        stats->paths = (uint64_t)cfg.W * cfg.H * cfg.spp;
+        stats->extension_rays = cnt[CNT_EXT];
+        stats->shadow_rays = cnt[CNT_SHADOW];
+        stats->reference_rays = cnt[CNT_REF];
+        stats->kernel_launches = 1;
+        stats->total_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return PGPU_OK;
 }
 
 static int32_t run_query(pgpu_ctx* c, int32_t id, bool camera, const float* in, int32_t n,
