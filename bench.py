@@ -186,17 +186,6 @@ def ncu_traffic_per_ray() -> float | None:
     return float(m.group(1)) if m else None
 
 
-def scene_bytes(scene) -> int:
-    """Bytes pgpu_upload_scene copies to the device: child-pair nodes, leaf
-    geometry (two float4), material and primitive ids, vertices, materials,
-    lights."""
-    n = scene.n_unified
-    n_tri = int((scene.prims["type"] == 1).sum()) + len(scene.mesh_indices)
-    verts = len(scene.mesh_vertices) + 3 * int((scene.prims["type"] == 1).sum())
-    return (max(n - 1, 0) * 64 + n * (16 + 16 + 4 + 4) + verts * 16 +
-            scene.n_materials * 64 + len(scene.lights) * 64) if n_tri >= 0 else 0
-
-
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -291,7 +280,9 @@ def run_ours(args) -> None:
     dominant = max(("extend", "shade", "shadow", "generate", "accumulate"), key=lambda k: kms[k])
     ext_launches = prof.kernel_launches and (prof.kernel_launches // max(1, 2 + 3 * st.pathtrace_bounces)) * st.pathtrace_bounces
     per_ray_queue = 16 + 16 + 16 + 4 + 16            # ray o, d, state, queue slot; hit write
-    alg_bytes = cnt.ext_node_visits * 64 + cnt.ext_leaf_bytes + cnt.extension_rays * per_ray_queue
+    wide_node_bytes = 7 * 16                         # 4-wide node: 6 planes x 4 boxes + refs
+    alg_bytes = (cnt.ext_node_visits * wide_node_bytes + cnt.ext_leaf_bytes +
+                 cnt.extension_rays * per_ray_queue)
     n_ext_launches = max(1, ext_launches)
     achieved = alg_bytes / (kms["extend"] * 1e-3) / 1e9
     peaks = measured_peaks()
@@ -313,7 +304,7 @@ def run_ours(args) -> None:
     if not args.no_e2e:
         host_img = torch.empty((st.height, st.width, 3), dtype=torch.float32).pin_memory()
         out_np = host_img.numpy()
-        h2d = scene_bytes(wl.scene)
+        h2d = ctx.scene_info(sid)["device_bytes"]   # the arena the upload copies
         d2h = out_np.nbytes
         ctx.render(sid, st, out=out_np)
         # Pencil builds its BVH when it parses the scene (ParsedScene::finalize);

@@ -294,6 +294,20 @@ int32_t pgpu_upload_scene(pgpu_ctx* ctx, const pgpu_scene* scene,
                           int32_t* out_scene_id);
 int32_t pgpu_free_scene(pgpu_ctx* ctx, int32_t scene_id);
 
+/* Sizes of an uploaded scene. No counterpart in the reference (Pencil keeps
+ * its scene on the host): it reports what pgpu_upload_scene built. */
+typedef struct pgpu_scene_info {
+    int64_t device_bytes;      /* bytes of the scene's device arena, all copied
+                                  from pinned host memory by the upload      */
+    int32_t n_leaves;          /* primitives (one per BVH leaf)              */
+    int32_t n_interior;        /* interior nodes of the binary tree          */
+    int32_t n_wide;            /* 4-wide nodes collapsed from it             */
+    int32_t bvh_depth;         /* levels of the binary tree                  */
+    int32_t wide_stack;        /* traversal stack entries the wide tree needs */
+    int32_t reserved;
+} pgpu_scene_info;
+int32_t pgpu_get_scene_info(pgpu_ctx* ctx, int32_t scene_id, pgpu_scene_info* out);
+
 /* Render one image: out_rgb gets width*height*3 floats, row-major, row 0 at
  * the top, each pixel the mean of its n*n samples (the layout of
  * Renderer::render's std::vector<Color>). out_m2 (optional) gets the

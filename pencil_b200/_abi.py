@@ -95,6 +95,12 @@ class Stats(C.Structure):
         return d
 
 
+class SceneInfo(C.Structure):
+    _fields_ = [("device_bytes", C.c_int64), ("n_leaves", C.c_int32),
+                ("n_interior", C.c_int32), ("n_wide", C.c_int32), ("bvh_depth", C.c_int32),
+                ("wide_stack", C.c_int32), ("reserved", C.c_int32)]
+
+
 EXPORTS = {
     "pgpu_abi_version": (C.c_int32, []),
     "pgpu_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p)]),
@@ -120,6 +126,7 @@ EXPORTS = {
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.POINTER(Stats)]),
     "pgpu_update_materials": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
+    "pgpu_get_scene_info": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(SceneInfo)]),
     "pgpu_render_noalloc": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(RenderParams),
                                         C.c_void_p, C.c_void_p]),
 }

@@ -53,6 +53,9 @@ struct DeviceScene {
     SceneView view{};
     int n_unified = 0;
     int n_leaves = 0;
+    int n_interior = 0;
+    int n_wide = 0;
+    int wide_stack = 0;
     int depth = 0;
     std::vector<DevMaterial> mats;
     std::vector<DevLight> lights;
@@ -418,8 +421,26 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     for (int k = 0; k < s->n_prims; ++k) n_explicit_tri += s->prims[k].type == PGPU_PRIM_TRIANGLE;
     const size_t n_verts = (size_t)s->n_mesh_vertices + 3 * (size_t)n_explicit_tri;
 
+    auto ref_of = [&](int k) -> int {
+        if (nodes[k].left >= 0) return idx[k];
+        int prim = nodes[k].right;
+        int type = prim < s->n_prims ? s->prims[prim].type : PGPU_PRIM_TRIANGLE;
+        return ~((type << kLeafTypeShift) | idx[k]);
+    };
+    // 4-wide nodes for the wavefront's traversal
+    std::vector<int> leaf_ref(n_nodes, 0);
+    for (int k = 0; k < n_nodes; ++k)
+        if (nodes[k].left < 0) leaf_ref[k] = ref_of(k);
+    std::vector<float4> wide;
+    int wide_stack = 0;
+    const int n_wide = collapse_wide(nodes, n_nodes, leaf_ref, kMaxDepth, wide, wide_stack);
+    if (wide_stack > kMaxDepth)
+        return fail(c, PGPU_ERR_UNSUPPORTED, "BVH needs %d stack entries, more than %d",
+                    wide_stack, kMaxDepth);
+
     size_t off_nodes = 0;
-    size_t off_ga = align256(off_nodes + (size_t)n_int * 64);
+    size_t off_wide = align256(off_nodes + (size_t)n_int * 64);
+    size_t off_ga = align256(off_wide + (size_t)n_wide * kWideNodeFloat4 * 16);
     size_t off_gb = align256(off_ga + (size_t)n_leaf * 16);
     size_t off_vt = align256(off_gb + (size_t)n_leaf * 16);
     size_t off_lm = align256(off_vt + n_verts * 16);
@@ -449,13 +470,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         h_vt[k] = make_float4(s->mesh_vertices[3 * k], s->mesh_vertices[3 * k + 1],
                               s->mesh_vertices[3 * k + 2], 0.0f);
     size_t next_vert = (size_t)s->n_mesh_vertices;
-
-    auto ref_of = [&](int k) -> int {
-        if (nodes[k].left >= 0) return idx[k];
-        int prim = nodes[k].right;
-        int type = prim < s->n_prims ? s->prims[prim].type : PGPU_PRIM_TRIANGLE;
-        return ~((type << kLeafTypeShift) | idx[k]);
-    };
+    if (n_wide) std::memcpy(host + off_wide, wide.data(), wide.size() * sizeof(float4));
     for (int k = 0; k < n_nodes; ++k) {
         const pgpu_bvh_node& nd = nodes[k];
         if (nd.left >= 0) {
@@ -526,6 +541,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     unsigned char* base = static_cast<unsigned char*>(ds->arena);
     SceneView& v = ds->view;
     v.nodes = reinterpret_cast<const float4*>(base + off_nodes);
+    v.wide = n_wide ? reinterpret_cast<const float4*>(base + off_wide) : nullptr;
     v.geo_a = reinterpret_cast<const float4*>(base + off_ga);
     v.geo_b = reinterpret_cast<const float4*>(base + off_gb);
     v.verts = reinterpret_cast<const float4*>(base + off_vt);
@@ -548,6 +564,9 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     std::memcpy(v.amb, s->ambient, 12);
     ds->n_unified = nU;
     ds->n_leaves = n_leaf;
+    ds->n_interior = n_int;
+    ds->n_wide = n_wide;
+    ds->wide_stack = wide_stack;
     ds->depth = depth;
     ds->mats = mats;
     ds->lights = lights;
@@ -566,6 +585,22 @@ int32_t pgpu_free_scene(pgpu_ctx* c, int32_t id) {
     cudaStreamSynchronize(c->stream);
     cudaFree(ds->arena);
     c->scenes.erase(id);
+    return PGPU_OK;
+}
+
+int32_t pgpu_get_scene_info(pgpu_ctx* c, int32_t id, pgpu_scene_info* out) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    if (!out) return fail(c, PGPU_ERR_INVALID_ARG, "null info pointer");
+    DeviceScene* ds = find_scene(c, id);
+    if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
+    pgpu_scene_info info{};
+    info.device_bytes = (int64_t)ds->bytes;
+    info.n_leaves = ds->n_leaves;
+    info.n_interior = ds->n_interior;
+    info.n_wide = ds->n_wide;
+    info.bvh_depth = ds->depth;
+    info.wide_stack = ds->wide_stack;
+    *out = info;
     return PGPU_OK;
 }
 

@@ -132,6 +132,20 @@ __device__ __forceinline__ RayPre prep(const Ray& r) {
     return p;
 }
 
+// Three-input min/max (PTX ISA 8.8, sm_100). Like fminf/fmaxf they ignore
+// NaN operands; min and max round nothing, so any grouping gives the same
+// value.
+__device__ __forceinline__ float fmax3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float fmin3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 // AABB::hit: sequential per-axis clipping with NaN-ignoring selects equals
 // clipping by the max of near distances and the min of far distances.
 // `entry` returns the clipped entry distance (independent of tmax).
@@ -144,8 +158,8 @@ __device__ __forceinline__ bool slab(float lox, float loy, float loz, float hix,
     float t1y = ((r.ny ? loy : hiy) - r.o.y) * r.inv.y;
     float t0z = ((r.nz ? hiz : loz) - r.o.z) * r.inv.z;
     float t1z = ((r.nz ? loz : hiz) - r.o.z) * r.inv.z;
-    float en = fmaxf(fmaxf(fmaxf(tmin, t0x), t0y), t0z);
-    float ex = fminf(fminf(fminf(tmax, t1x), t1y), t1z);
+    float en = fmax3f(fmaxf(tmin, t0x), t0y, t0z);
+    float ex = fmin3f(fminf(tmax, t1x), t1y, t1z);
     entry = en;
     return !(ex < en);
 }
@@ -632,6 +646,212 @@ struct AnyTrav {
         }
         if (hL) { node = rr.x; return false; }
         if (hR) { node = rr.y; return false; }
+        if (sp == 0) return true;
+        --sp;
+        float te;
+        stk.pop(sp, node, te);
+        return false;
+    }
+};
+
+// ---- 4-wide traversal (wavefront) ------------------------------------------------
+// One wide node: its four child boxes (SoA float4 per plane) and refs.
+struct WideNode {
+    float4 lx, ly, lz, hx, hy, hz;
+    int4 ref;
+};
+__device__ __forceinline__ WideNode load_wide(const float4* wide, int node) {
+    const float4* np = wide + (size_t)kWideNodeFloat4 * node;
+    WideNode w;
+    w.lx = __ldg(np);
+    w.ly = __ldg(np + 1);
+    w.lz = __ldg(np + 2);
+    w.hx = __ldg(np + 3);
+    w.hy = __ldg(np + 4);
+    w.hz = __ldg(np + 5);
+    w.ref = __ldg(reinterpret_cast<const int4*>(np + 6));
+    return w;
+}
+
+// Slab tests of the four children: bit k of the result is child k's hit,
+// e[k] its entry distance.
+__device__ __forceinline__ unsigned slab4(const WideNode& w, const RayPre& r, float tmin,
+                                          float tmax, float (&e)[4]) {
+    unsigned m = 0;
+    m |= slab(w.lx.x, w.ly.x, w.lz.x, w.hx.x, w.hy.x, w.hz.x, r, tmin, tmax, e[0]) ? 1u : 0u;
+    m |= slab(w.lx.y, w.ly.y, w.lz.y, w.hx.y, w.hy.y, w.hz.y, r, tmin, tmax, e[1]) ? 2u : 0u;
+    m |= slab(w.lx.z, w.ly.z, w.lz.z, w.hx.z, w.hy.z, w.hz.z, r, tmin, tmax, e[2]) ? 4u : 0u;
+    m |= slab(w.lx.w, w.ly.w, w.lz.w, w.hx.w, w.hy.w, w.hz.w, r, tmin, tmax, e[3]) ? 8u : 0u;
+    return m;
+}
+
+// Child k's ref / entry distance by a select chain (no local-memory indexing).
+__device__ __forceinline__ int pick_ref(const int4& r, int k) {
+    return k == 0 ? r.x : k == 1 ? r.y : k == 2 ? r.z : r.w;
+}
+__device__ __forceinline__ float pick_e(const float (&e)[4], int k) {
+    return k == 0 ? e[0] : k == 1 ? e[1] : k == 2 ? e[2] : e[3];
+}
+// Children of a wide node whose ref is a leaf, as bits.
+__device__ __forceinline__ unsigned leaf_bits(const int4& r) {
+    return (r.x < 0 ? 1u : 0u) | (r.y < 0 ? 2u : 0u) | (r.z < 0 ? 4u : 0u) | (r.w < 0 ? 8u : 0u);
+}
+
+// Resumable closest-hit traversal of the 4-wide tree. Same result rule as
+// ClosestTrav (smallest t, ties to the later DFS leaf); children are taken
+// nearest first, the others stacked with their entry distance.
+template <int kShared, bool COUNT>
+struct ClosestTrav4 {
+    Ray ray;
+    RayPre rp;
+    float tmin, t_best;
+    int best, best_ref;
+    int node, sp;
+
+    __device__ __forceinline__ void test_leaf(const SceneView& S, int ref, TravCount* cnt) {
+        float t;
+        if (COUNT) { cnt->prims++; cnt->leaf_bytes += leaf_bytes(ref); }
+        if (hit_leaf<false>(S, ref, ray, tmin, t_best, t, nullptr)) {
+            int slot = (~ref) & kLeafSlotMask;
+            if (t < t_best || slot > best) { t_best = t; best = slot; best_ref = ref; }
+        }
+    }
+
+    __device__ __forceinline__ bool init(const SceneView& S, const Ray& r, float tmin_,
+                                         float tmax, TravCount* cnt) {
+        ray = r;
+        tmin = tmin_;
+        t_best = tmax;
+        best = -1;
+        best_ref = 0;
+        sp = 0;
+        node = 0;
+        if (S.root_ref == kEmptyRoot) return true;
+        rp = prep(r);
+        float e;
+        if (!slab(S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1],
+                  S.root_max[2], rp, tmin, tmax, e))
+            return true;
+        if (S.root_ref < 0) {
+            test_leaf(S, S.root_ref, cnt);
+            return true;
+        }
+        return false;
+    }
+
+    __device__ __forceinline__ bool step(const SceneView& S, TravStack<kShared>& stk,
+                                         TravCount* cnt) {
+        const WideNode w = load_wide(S.wide, node);
+        if (COUNT) cnt->nodes++;
+        float e[4];
+        unsigned m = slab4(w, rp, tmin, t_best, e);
+        unsigned lm = m & leaf_bits(w.ref);
+        m &= ~lm;
+        while (lm) {
+            const int k = __ffs(lm) - 1;
+            lm &= lm - 1;
+            if (pick_e(e, k) <= t_best) test_leaf(S, pick_ref(w.ref, k), cnt);
+        }
+        // interior children still in reach, nearest first (sorting network)
+        float k0 = (m & 1u) && e[0] <= t_best ? e[0] : INFINITY;
+        float k1 = (m & 2u) && e[1] <= t_best ? e[1] : INFINITY;
+        float k2 = (m & 4u) && e[2] <= t_best ? e[2] : INFINITY;
+        float k3 = (m & 8u) && e[3] <= t_best ? e[3] : INFINITY;
+        int r0 = w.ref.x, r1 = w.ref.y, r2 = w.ref.z, r3 = w.ref.w;
+        auto cs = [](float& ka, int& ra, float& kb, int& rb) {
+            const bool sw = kb < ka;
+            const float tk = ka;
+            const int tr = ra;
+            ka = sw ? kb : ka;
+            ra = sw ? rb : ra;
+            kb = sw ? tk : kb;
+            rb = sw ? tr : rb;
+        };
+        cs(k0, r0, k1, r1);
+        cs(k2, r2, k3, r3);
+        cs(k0, r0, k2, r2);
+        cs(k1, r1, k3, r3);
+        cs(k1, r1, k2, r2);
+        if (k0 != INFINITY) {
+            if (k3 != INFINITY) stk.push(sp++, r3, k3);
+            if (k2 != INFINITY) stk.push(sp++, r2, k2);
+            if (k1 != INFINITY) stk.push(sp++, r1, k1);
+            node = r0;
+            return false;
+        }
+        while (sp > 0) {
+            --sp;
+            int ref;
+            float te;
+            stk.pop(sp, ref, te);
+            if (te <= t_best) { node = ref; return false; }
+        }
+        return true;
+    }
+};
+
+// Resumable any-hit traversal of the 4-wide tree (BVHNode::occluded,
+// src/bvh.hpp:39-48): with a fixed t_max the set of boxes entered does not
+// depend on the order, so the answer equals the reference's.
+template <int kShared, bool COUNT>
+struct AnyTrav4 {
+    Ray ray;
+    RayPre rp;
+    float tmin, tmax;
+    int node, sp;
+    bool hit;
+
+    __device__ __forceinline__ bool test_leaf(const SceneView& S, int ref, TravCount* cnt) {
+        float t;
+        if (COUNT) { cnt->prims++; cnt->leaf_bytes += leaf_bytes(ref); }
+        return hit_leaf<false>(S, ref, ray, tmin, tmax, t, nullptr);
+    }
+
+    __device__ __forceinline__ bool init(const SceneView& S, const Ray& r, float tmin_,
+                                         float tmax_, TravCount* cnt) {
+        ray = r;
+        tmin = tmin_;
+        tmax = tmax_;
+        hit = false;
+        sp = 0;
+        node = 0;
+        if (S.root_ref == kEmptyRoot) return true;
+        rp = prep(r);
+        float e;
+        if (!slab(S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1],
+                  S.root_max[2], rp, tmin, tmax, e))
+            return true;
+        if (S.root_ref < 0) {
+            hit = test_leaf(S, S.root_ref, cnt);
+            return true;
+        }
+        return false;
+    }
+
+    __device__ __forceinline__ bool step(const SceneView& S, TravStack<kShared>& stk,
+                                         TravCount* cnt) {
+        const WideNode w = load_wide(S.wide, node);
+        if (COUNT) cnt->nodes++;
+        float e[4];
+        unsigned m = slab4(w, rp, tmin, tmax, e);
+        unsigned lm = m & leaf_bits(w.ref);
+        m &= ~lm;
+        while (lm) {
+            const int k = __ffs(lm) - 1;
+            lm &= lm - 1;
+            if (test_leaf(S, pick_ref(w.ref, k), cnt)) { hit = true; return true; }
+        }
+        if (m) {
+            const int k = __ffs(m) - 1;
+            m &= m - 1;
+            while (m) {
+                const int j = __ffs(m) - 1;
+                m &= m - 1;
+                stk.push(sp++, pick_ref(w.ref, j), 0.0f);
+            }
+            node = pick_ref(w.ref, k);
+            return false;
+        }
         if (sp == 0) return true;
         --sp;
         float te;

@@ -17,6 +17,14 @@ void build_bvh(const std::vector<pgpu_prim>& prims, std::vector<pgpu_bvh_node>& 
 int make_prim(int type, int material, const float* a, const float* b, const float* c, float s0,
               float s1, pgpu_prim* out);
 
+// bvh_wide.cpp: 4-wide nodes (kWideNodeFloat4 float4 each) collapsed from a
+// validated binary tree in DFS pre-order. leaf_ref[k] is the leaf ref of
+// binary leaf k. Returns the number of wide nodes (0 when the root is a
+// leaf); stack_need receives the most stack entries a traversal holds, which
+// is at most max_stack unless the binary tree itself needs more.
+int collapse_wide(const pgpu_bvh_node* nodes, int n_nodes, const std::vector<int>& leaf_ref,
+                  int max_stack, std::vector<float4>& out, int& stack_need);
+
 // Render configuration after validation.
 struct RenderCfg {
     int W, H, n, spp, depth, mode, engine, rng, glass, soft;

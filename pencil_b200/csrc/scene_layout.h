@@ -12,6 +12,13 @@
 //             [4i+2] = (R.min.z, R.max.x, R.max.y, R.max.z)
 //             [4i+3] = (ref L, ref R, -, -)            (int bits)
 //           ref >= 0: interior node index; ref < 0: leaf, ~ref = type<<28 | slot
+//   wide    float4[8 * n_wide]      4-wide nodes collapsed from the same tree
+//                                   (bvh_wide.cpp), used by the wavefront:
+//             [8i+0..2] = min.x, min.y, min.z of children 0..3
+//             [8i+3..5] = max.x, max.y, max.z of children 0..3
+//             [8i+6]    = refs of children 0..3 (int bits; a missing child
+//                         has an empty box and a leaf ref of type LEAF_NONE)
+//             [8i+7]    = unused
 //   geo_a   float4[n_leaves]        leaf geometry in DFS leaf order (slot):
 //             sphere   (center.xyz, radius)
 //             triangle (i0, i1, i2, -)  int bits, indices into verts
@@ -48,7 +55,10 @@ enum LeafType : int {
     LEAF_PLANE = 3,
     LEAF_CYLINDER = 4,
     LEAF_CONE = 5,
+    LEAF_NONE = 7,          // placeholder child of a wide node: never hit
 };
+constexpr int kLeafNone = LEAF_NONE;
+constexpr int kWideNodeFloat4 = 8;
 
 constexpr int kLeafTypeShift = 28;
 constexpr int kLeafSlotMask = (1 << kLeafTypeShift) - 1;
@@ -82,6 +92,7 @@ struct alignas(16) DevLight {
 // single-scene launches and read from global memory for batched ones.
 struct SceneView {
     const float4* nodes;
+    const float4* wide;    // 4-wide nodes (null when the root is a leaf)
     const float4* geo_a;
     const float4* geo_b;
     const float4* verts;

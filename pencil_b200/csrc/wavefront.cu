@@ -214,7 +214,7 @@ wf_extend(WfArgs A, int it) {
     unsigned int* cursor = A.work + it * 3 + 0;
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    ClosestTrav<kWfShared, COUNT> tr;
+    ClosestTrav4<kWfShared, COUNT> tr;
     const SceneView* S = nullptr;
     int slot = -1;
     bool active = false;
@@ -373,7 +373,7 @@ wf_shadow(WfArgs A, int it) {
     unsigned int* cursor = A.work + it * 3 + 2;
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    AnyTrav<kWfShared, COUNT> tr;
+    AnyTrav4<kWfShared, COUNT> tr;
     const SceneView* S = nullptr;
     NeeAccum acc;
     V3 L = v3(0, 0, 0), c = v3(0, 0, 0);

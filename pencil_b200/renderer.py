@@ -141,6 +141,15 @@ class GpuContext:
     def free(self, sid: int) -> None:
         self.check(self.lib.pgpu_free_scene(self.h, sid), "pgpu_free_scene")
 
+    def scene_info(self, sid: int) -> dict:
+        """Sizes of an uploaded scene (device bytes, leaves, binary and wide
+        node counts, depth, wide-tree stack need)."""
+        info = A.SceneInfo()
+        self.check(self.lib.pgpu_get_scene_info(self.h, sid, C.byref(info)),
+                   "pgpu_get_scene_info")
+        return {name: int(getattr(info, name)) for name, _ in A.SceneInfo._fields_
+                if name != "reserved"}
+
     def update_materials(self, sid: int, mats: np.ndarray) -> None:
         mats = np.ascontiguousarray(mats, A.MATERIAL_DTYPE)
         self.check(self.lib.pgpu_update_materials(self.h, sid, A.ptr(mats), len(mats)),

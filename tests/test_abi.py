@@ -36,6 +36,7 @@ def test_abi_version_and_record_sizes():
     assert C.sizeof(A.Camera) == 52
     assert C.sizeof(A.RenderParams) == 64
     assert C.sizeof(A.Stats) == 152
+    assert C.sizeof(A.SceneInfo) == 32
 
 
 def test_null_context_is_rejected():
@@ -46,6 +47,7 @@ def test_null_context_is_rejected():
     p = A.RenderParams()
     assert lib.pgpu_render(None, 1, C.byref(p), None, None, None) == A.ERR_INVALID_ARG
     assert lib.pgpu_free_scene(None, 1) == A.ERR_INVALID_ARG
+    assert lib.pgpu_get_scene_info(None, 1, None) == A.ERR_INVALID_ARG
     assert lib.pgpu_last_error(None) == b"null context"
     assert lib.pgpu_set_stream(None, None) == A.ERR_INVALID_ARG
 
