@@ -215,7 +215,9 @@ def run_ours(args) -> None:
     # (outside the timed region)
     from pencil_b200.autotune import autotune
     tuned = autotune(ctx, [sid], [st], scene=wl.scene, use_cache=False)
-    tuned = {k: tuned[k] for k in ("queue_capacity", "refill_below", "sort_key", "ms")}
+    tuned = {**{k: tuned[k] for k in ("queue_capacity", "refill_below", "sort_key", "ms")},
+             "trials": [[t["queue_capacity"], t["refill_below"], t["sort_key"], round(t["ms"], 3)]
+                        for t in tuned.get("trials", [])]}
 
     def barrier():
         torch.cuda.synchronize()

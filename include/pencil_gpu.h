@@ -229,7 +229,9 @@ typedef struct pgpu_render_params {
     int32_t  refill_below;      /* wavefront: a warp takes new rays once at
                                    most this many of its 32 lanes are still
                                    traversing (0: automatic)                 */
-    int32_t  sort_key;          /* wavefront ray-sort key (0: none)          */
+    int32_t  sort_key;          /* wavefront ray order: 0 queue order, 1 binned
+                                   by direction octant, 2 sorted by origin
+                                   (Morton code) and direction octant        */
 } pgpu_render_params;
 
 typedef struct pgpu_stats {

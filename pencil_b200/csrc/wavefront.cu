@@ -16,6 +16,8 @@
 // compacts surviving paths into the next queue with one atomic per warp
 // (ballot + popc), optionally binned by the octant of the new ray direction
 // (sort key 1) so that warps traverse with matching near/far child order.
+// Sort key 2 instead orders each iteration's shadow work by where its first
+// shadow ray starts (a counting sort over Morton cells and octants).
 // Next-event shadow rays are stored per slot and resolved by shadow in the
 // order shade made them, with the same NeeAccum as the megakernel, so each
 // path's radiance is bit-identical to the megakernel's. The whole frame is
@@ -36,6 +38,12 @@ constexpr int kWfShared = 16;
 constexpr int kWfBlock = 128;
 constexpr int kOctants = 8;
 constexpr int kDefaultRefill = 20;   // lanes still busy when a warp refetches
+// Sort key 2: each iteration's shadow work ordered by the Morton code of the
+// first shadow ray's origin (6 bits per axis of the scene's root box) and its
+// direction octant, so that a warp's shadow rays start close together and
+// traverse alike (2^21 bins; a counting sort per iteration).
+constexpr int kMortonBits = 6;
+constexpr int kSortBins = 1 << (3 * kMortonBits + 3);
 
 // One render job of the path space.
 struct WfJob {
@@ -75,7 +83,40 @@ struct WfArgs {
     int sort_key;
     int refill_below;         // extend/shadow: a warp refetches rays once at most
                               // this many of its lanes are still traversing
+    // sort key 2 (counting sort of each iteration's shadow work by sort_key_of):
+    int* key_s;               // [slot] key of the slot's first shadow ray
+    int* tmp_s;               // unsorted slots with shadow work
+    int* qs;                  // the same slots sorted by key
+    int* hist_s;              // kSortBins counters, then local bin offsets
+    int* chunk_off;           // kSortBins / 1024 chunk totals, then chunk offsets
+    int* tcnt;                // [iteration * 2 + 1] slots with shadow work
 };
+
+// Sort key of a ray: Morton code of its origin in the scene's root box
+// (kMortonBits per axis), then the octant of its direction.
+__device__ __forceinline__ uint32_t spread_bits3(uint32_t x) {
+    x &= 0x3ffu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+__device__ __forceinline__ int sort_key_of(const SceneView& S, V3 o, V3 d) {
+    const float cells = (float)(1 << kMortonBits);
+    uint32_t c[3];
+    const float oo[3] = {o.x, o.y, o.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float ext = S.root_max[a] - S.root_min[a];
+        const float f = ext > 0.0f ? (oo[a] - S.root_min[a]) * (cells / ext) : 0.0f;
+        const int q = f > 0.0f ? (int)f : 0;   // NaN and below the box: cell 0
+        c[a] = (uint32_t)min(q, (1 << kMortonBits) - 1);
+    }
+    const uint32_t m = spread_bits3(c[0]) | (spread_bits3(c[1]) << 1) | (spread_bits3(c[2]) << 2);
+    const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    return (int)((m << 3) | oct);
+}
 
 __device__ __forceinline__ int find_job(const WfJob* jobs, int n, long long path) {
     int lo = 0, hi = n - 1;
@@ -119,31 +160,36 @@ __device__ __forceinline__ void flush_counts(const WfArgs& A, const RayCount& rc
 }
 
 // Number of entries in iteration `it`'s queue and the queue entry -> slot map
-// across octant bins.
+// across octant bins. The bin counts are staged in shared memory, once per
+// block, so that the persistent loops hold no registers for them.
 struct QView {
     const int* q;
+    const int* cnt;   // shared: kOctants bin counts
     int Q;
-    int cnt[kOctants];
     int total;
     __device__ __forceinline__ int slot(int e) const {
         int b = 0;
-#pragma unroll
-        for (int k = 0; k < kOctants - 1; ++k) {
-            if (e >= cnt[b]) { e -= cnt[b]; ++b; }
+#pragma unroll 1
+        for (; b < kOctants - 1; ++b) {
+            const int c = cnt[b];
+            if (e < c) break;
+            e -= c;
         }
-        return q[b * Q + e];
+        return q[(size_t)b * Q + e];
     }
 };
+// Every thread of the block calls this (it synchronises the block once).
 __device__ __forceinline__ QView qview(const WfArgs& A, int it) {
+    __shared__ int s_cnt[kOctants];
+    if (threadIdx.x < kOctants) s_cnt[threadIdx.x] = A.counts[it * kOctants + threadIdx.x];
+    __syncthreads();
     QView v;
     v.q = A.q[it & 1];
+    v.cnt = s_cnt;
     v.Q = A.Q;
     v.total = 0;
 #pragma unroll
-    for (int k = 0; k < kOctants; ++k) {
-        v.cnt[k] = A.counts[it * kOctants + k];
-        v.total += v.cnt[k];
-    }
+    for (int k = 0; k < kOctants; ++k) v.total += s_cnt[k];
     return v;
 }
 
@@ -256,6 +302,17 @@ wf_extend(WfArgs A, int it) {
     flush_counts<COUNT>(A, rc, 1);
 }
 
+// Warp-aggregated append of `slot` where `take`: one atomic per warp.
+__device__ __forceinline__ void warp_append(bool take, int slot, int* counter, int* list,
+                                            int lane) {
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (!m) return;
+    int first = 0;
+    if (lane == __ffs(m) - 1) first = atomicAdd(counter, __popc(m));
+    first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
+    if (take) list[first + __popc(m & ((1u << lane) - 1u))] = slot;
+}
+
 // ---- shade --------------------------------------------------------------------
 // Emitter that stores a vertex's shadow records and pending terms per slot.
 struct StoreNee {
@@ -265,9 +322,10 @@ struct StoreNee {
     int kind;
     V3 base, tail, w;
     float s;
+    V3 o0, d0;                // first shadow ray (the sort key of the slot's shadow work)
     __device__ StoreNee(const WfArgs& a, int sl)
         : A(a), slot(sl), n(0), kind(0), base(v3(0, 0, 0)), tail(v3(0, 0, 0)), w(v3(0, 0, 0)),
-          s(0.0f) {}
+          s(0.0f), o0(v3(0, 0, 0)), d0(v3(0, 0, 0)) {}
     __device__ __forceinline__ void begin_none() { kind = 0; }
     __device__ __forceinline__ void begin_pt() { kind = 1; }
     __device__ __forceinline__ void begin_whitted(V3 b) { kind = 2; base = b; }
@@ -278,6 +336,7 @@ struct StoreNee {
             return;
         }
         size_t k = (size_t)n * A.Q + slot;
+        if (n == 0) { o0 = r.o; d0 = r.d; }
         A.sh_o[k] = make_float4(r.o.x, r.o.y, r.o.z, tmin);
         A.sh_d[k] = make_float4(r.d.x, r.d.y, r.d.z, tmax);
         A.sh_c[k] = make_float4(c.x, c.y, c.z, __int_as_float((test ? 1 : 0) | (group_end << 1)));
@@ -305,8 +364,10 @@ wf_shade(WfArgs A, int it) {
         if (base >= qv.total) break;
         int e = base + lane;
         bool alive = false;
+        bool shadow_work = false;
         int slot = -1;
         int bin = 0;
+        int key = -1;
         if (e < qv.total) {
             slot = qv.slot(e);
             uint4 stv = A.st[slot];
@@ -328,6 +389,11 @@ wf_shade(WfArgs A, int it) {
             StoreNee E(A, slot);
             alive = shade_vertex(S, J.P, ps, found, h, E);
             E.store();
+            shadow_work = E.kind != 0;
+            if (A.sort_key == 2 && shadow_work) {
+                key = sort_key_of(S, E.o0, E.d0);
+                A.key_s[slot] = key;
+            }
             if (COUNT && alive && (ps.flags & kFlagWhitted)) rc.ref++;
             A.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 0.0f);
             if (alive) {
@@ -339,6 +405,14 @@ wf_shade(WfArgs A, int it) {
                     bin = (ps.ray.d.x < 0.0f ? 1 : 0) | (ps.ray.d.y < 0.0f ? 2 : 0) |
                           (ps.ray.d.z < 0.0f ? 4 : 0);
             }
+        }
+        // sort key 2: the unsorted list of slots with shadow work, ordered by
+        // wf_sort_scatter
+        if (A.sort_key == 2) {
+            warp_append(shadow_work, slot, A.tcnt + 2 * it + 1, A.tmp_s, lane);
+            // bin counts, one atomic per distinct key in the warp
+            const unsigned same = __match_any_sync(0xffffffffu, key);
+            if (shadow_work && lane == __ffs(same) - 1) atomicAdd(A.hist_s + key, __popc(same));
         }
         // warp-aggregated append, one atomic per (warp, bin)
         const int nbins = A.sort_key == 1 ? kOctants : 1;
@@ -353,6 +427,92 @@ wf_shade(WfArgs A, int it) {
         }
     }
     flush_counts<COUNT>(A, rc);
+}
+
+// ---- sort key 2: counting sort of shade's shadow-work list ----------------------
+// The bin counts are scanned in chunks of kSortChunk bins: wf_sort_scan turns
+// each chunk into local exclusive offsets and its total into chunk_off;
+// wf_sort_chunks scans the chunk totals. A slot's position is then
+// chunk_off[key / kSortChunk] plus its bin's running local offset.
+constexpr int kSortChunk = 1024;
+constexpr int kSortChunks = kSortBins / kSortChunk;
+
+// Exclusive scan of one value per thread of a 1024-thread block; returns the
+// block total through *total.
+__device__ __forceinline__ int block_scan_1024(int v, int* s_warp, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = s_warp[lane];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, off);
+            if (lane >= off) w += y;
+        }
+        s_warp[lane] = w;
+    }
+    __syncthreads();
+    *total = s_warp[31];
+    return x - v + (warp ? s_warp[warp - 1] : 0);
+}
+
+__global__ void __launch_bounds__(kSortChunk) wf_sort_scan(WfArgs A) {
+    __shared__ int s_warp[32];
+    int* h = A.hist_s + (size_t)blockIdx.x * kSortChunk;
+    int total = 0;
+    const int ex = block_scan_1024(h[threadIdx.x], s_warp, &total);
+    h[threadIdx.x] = ex;
+    if (threadIdx.x == 0) A.chunk_off[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kSortChunk) wf_sort_chunks(WfArgs A) {
+    __shared__ int s_warp[32];
+    constexpr int per = (kSortChunks + kSortChunk - 1) / kSortChunk;
+    int v[per];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < per; ++k) {
+        const int c = threadIdx.x * per + k;
+        v[k] = c < kSortChunks ? A.chunk_off[c] : 0;
+        sum += v[k];
+    }
+    int total = 0;
+    int run = block_scan_1024(sum, s_warp, &total);
+#pragma unroll
+    for (int k = 0; k < per; ++k) {
+        const int c = threadIdx.x * per + k;
+        if (c < kSortChunks) A.chunk_off[c] = run;
+        run += v[k];
+    }
+}
+
+// Places every listed slot at its bin's next position (the order inside a
+// bin is arbitrary; a path's result does not depend on its queue position).
+__global__ void __launch_bounds__(kWfBlock) wf_sort_scatter(WfArgs A, int it) {
+    const int ns = A.tcnt[2 * it + 1];
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    // whole warps iterate together (the key match below needs every lane)
+    for (int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); e0 < ns; e0 += stride) {
+        const int e = e0 + lane;
+        const bool on = e < ns;
+        const int slot = on ? A.tmp_s[e] : -1;
+        const int key = on ? A.key_s[slot] : -1;
+        const unsigned same = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(same) - 1;
+        int base = 0;
+        if (on && lane == leader)
+            base = A.chunk_off[key / kSortChunk] + atomicAdd(A.hist_s + key, __popc(same));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (on) A.qs[base + __popc(same & ((1u << lane) - 1u))] = slot;
+    }
 }
 
 // ---- shadow -------------------------------------------------------------------
@@ -370,6 +530,9 @@ wf_shadow(WfArgs A, int it) {
     stk.stride = blockDim.x;
     RayCount rc = {};
     const QView qv = qview(A, it);
+    // sort key 2: the slots with shadow work, sorted by their first shadow ray
+    const bool sorted = A.sort_key == 2;
+    const int total = sorted ? A.tcnt[2 * it + 1] : qv.total;
     unsigned int* cursor = A.work + it * 3 + 2;
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
@@ -415,11 +578,11 @@ wf_shadow(WfArgs A, int it) {
             int base = 0;
             if (lane == 0) base = (int)atomicAdd(cursor, (unsigned)__popc(idle));
             base = __shfl_sync(0xffffffffu, base, 0);
-            if (base + __popc(idle) >= qv.total) exhausted = true;
+            if (base + __popc(idle) >= total) exhausted = true;
             if (!active) {
                 const int e = base + __popc(idle & below);
-                if (e < qv.total) {
-                    slot = qv.slot(e);
+                if (e < total) {
+                    slot = sorted ? A.qs[e] : qv.slot(e);
                     const int kind = __float_as_int(A.pw[slot].w);
                     if (kind != 0) {
                         S = &A.views[A.jobs[A.st[slot].w].view];
@@ -543,6 +706,10 @@ static cudaError_t ensure_scratch(WfScratch& W, int Q, int maxS, int iters, int 
     sz += al((size_t)(iters + 2) * kOctants * 4);    // counts
     sz += al((size_t)(iters + 2) * 3 * 4);           // work cursors
     sz += al(4);                                     // status
+    sz += 3 * al((size_t)Q * 4);                     // sort: keys, list, shadow queue
+    sz += al((size_t)kSortBins * 4);                 // sort: bin histogram
+    sz += al((size_t)kSortChunks * 4);               // sort: chunk offsets
+    sz += al((size_t)(iters + 2) * 2 * 4);           // sort: list counts
     sz += al((size_t)n_views * sizeof(SceneView));
     sz += al((size_t)n_jobs * sizeof(WfJob));
     cudaError_t e = cudaMalloc(&W.mem, sz);
@@ -575,6 +742,12 @@ static cudaError_t ensure_scratch(WfScratch& W, int Q, int maxS, int iters, int 
     A.counts = reinterpret_cast<int*>(take((size_t)(iters + 2) * kOctants * 4));
     A.work = reinterpret_cast<unsigned int*>(take((size_t)(iters + 2) * 3 * 4));
     A.status = reinterpret_cast<int*>(take(4));
+    A.key_s = reinterpret_cast<int*>(take((size_t)Q * 4));
+    A.tmp_s = reinterpret_cast<int*>(take((size_t)Q * 4));
+    A.qs = reinterpret_cast<int*>(take((size_t)Q * 4));
+    A.hist_s = reinterpret_cast<int*>(take((size_t)kSortBins * 4));
+    A.chunk_off = reinterpret_cast<int*>(take((size_t)kSortChunks * 4));
+    A.tcnt = reinterpret_cast<int*>(take((size_t)(iters + 2) * 2 * 4));
     W.d_views = reinterpret_cast<SceneView*>(take((size_t)n_views * sizeof(SceneView)));
     W.d_jobs = reinterpret_cast<WfJob*>(take((size_t)n_jobs * sizeof(WfJob)));
     A.views = W.d_views;
@@ -595,7 +768,7 @@ static int max_shadow_records(const SceneView& v, const std::vector<DevLight>& l
 }
 
 struct WfOccupancy {
-    int grid_extend = 0, grid_shade = 0, grid_shadow = 0;
+    int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_scatter = 0;
 };
 
 template <bool COUNT>
@@ -611,6 +784,7 @@ static cudaError_t occupancy(WfOccupancy& o) {
     o.grid_extend = sms * std::max(b1, 1);
     o.grid_shade = sms * std::max(b2, 1);
     o.grid_shadow = sms * std::max(b3, 1);
+    o.grid_scatter = sms * 8;
     return e;
 }
 
@@ -674,6 +848,9 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         size_t cnt_bytes = (size_t)(iters + 2) * kOctants * 4;
         if ((e = cudaMemsetAsync(A.counts, 0, cnt_bytes, st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(A.work, 0, (size_t)(iters + 2) * 3 * 4, st)) != cudaSuccess) return e;
+        if (A.sort_key == 2 &&
+            (e = cudaMemsetAsync(A.tcnt, 0, (size_t)(iters + 2) * 2 * 4, st)) != cudaSuccess)
+            return e;
         int gblocks = (int)((slots + kWfBlock - 1) / kWfBlock);
         lt.mark(KC_GENERATE, st, true);
         wf_generate<COUNT><<<gblocks, kWfBlock, 0, st>>>(A, path_begin, (int)slots);
@@ -684,7 +861,17 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
             wf_extend<COUNT><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
             lt.mark(KC_EXTEND, st, false);
             lt.mark(KC_SHADE, st, true);
+            if (A.sort_key == 2) {
+                if ((e = cudaMemsetAsync(A.hist_s, 0, (size_t)kSortBins * 4, st)) != cudaSuccess)
+                    return e;
+            }
             wf_shade<COUNT><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
+            if (A.sort_key == 2) {
+                wf_sort_scan<<<kSortChunks, kSortChunk, 0, st>>>(A);
+                wf_sort_chunks<<<1, kSortChunk, 0, st>>>(A);
+                wf_sort_scatter<<<occ.grid_scatter, kWfBlock, 0, st>>>(A, it);
+                n_launch += 3;
+            }
             lt.mark(KC_SHADE, st, false);
             lt.mark(KC_SHADOW, st, true);
             wf_shadow<COUNT><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
