@@ -207,8 +207,10 @@ enum pgpu_flags {
     PGPU_FLAG_COUNT_NODES   = 4,  /* also count node visits / prim tests    */
     PGPU_FLAG_NO_GRAPH      = 8,  /* wavefront: launch kernels one by one
                                      instead of replaying a CUDA graph       */
-    PGPU_FLAG_PROFILE_KERNELS = 16 /* time each kernel class (implies
+    PGPU_FLAG_PROFILE_KERNELS = 16, /* time each kernel class (implies
                                      NO_GRAPH); see pgpu_stats.kernel_ms     */
+    PGPU_FLAG_NO_PACKETS    = 32  /* wavefront: trace camera rays one per lane
+                                     instead of as warp packets              */
 };
 
 typedef struct pgpu_render_params {

@@ -682,6 +682,7 @@ int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, Re
         return fail(c, PGPU_ERR_INVALID_ARG, "sort_key must be 0, 1 or 2");
     cfg.sort_key = p->sort_key;
     cfg.profile = (p->flags & PGPU_FLAG_PROFILE_KERNELS) != 0;
+    cfg.packets = (p->flags & PGPU_FLAG_NO_PACKETS) == 0;
     (void)ds;
     return PGPU_OK;
 }

@@ -36,6 +36,7 @@ struct RenderCfg {
     int queue_capacity;
     int sort_key;
     bool profile;
+    bool packets;     // wavefront: camera rays of a one-scene frame as warp packets
 };
 
 // Device counters written by the kernels (atomic adds).

@@ -81,6 +81,7 @@ struct WfArgs {
     int* status;              // 1: shadow record overflow
     unsigned long long* counters;
     int sort_key;
+    int packets;              // 1: the first bounce of a one-scene frame as warp packets
     int refill_below;         // extend/shadow: a warp refetches rays once at most
                               // this many of its lanes are still traversing
     // sort key 2 (counting sort of each iteration's shadow work by sort_key_of):
@@ -311,6 +312,106 @@ __device__ __forceinline__ void warp_append(bool take, int slot, int* counter, i
     if (lane == __ffs(m) - 1) first = atomicAdd(counter, __popc(m));
     first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
     if (take) list[first + __popc(m & ((1u << lane) - 1u))] = slot;
+}
+
+// ---- extend, camera rays of one scene: warp packets ------------------------------
+// The first bounce's queue holds the camera rays in slot order, so a warp's
+// 32 rays are the samples of two neighbouring pixels: nearly the same ray.
+// The warp traverses the 4-wide tree once for all of them: every lane tests
+// every node the packet enters against its own ray and its own t_best, the
+// packet enters a child that any lane still reaches (nearest first by the
+// lanes' smallest entry distance), and one shared stack serves the warp.
+// Node loads are broadcasts and all lanes stay busy. A lane still tests a
+// leaf only when its own slab test reaches it, so its result is the closest
+// hit among the same leaves as its own traversal would test.
+template <bool COUNT>
+__global__ void __launch_bounds__(kWfBlock) wf_extend_packet(WfArgs A) {
+    __shared__ int s_ref[kWfBlock / 32][kMaxStack];
+    __shared__ float s_key[kWfBlock / 32][kMaxStack];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int* sref = s_ref[warp];
+    float* skey = s_key[warp];
+    RayCount rc = {};
+    const QView qv = qview(A, 0);
+    unsigned int* cursor = A.work + 0;
+    const SceneView& S = A.views[A.jobs[0].view];
+    while (true) {
+        const int base = fetch32(cursor);
+        if (base >= qv.total) break;
+        const int e = base + lane;
+        const bool valid = e < qv.total;
+        const int slot = valid ? qv.slot(e) : -1;
+        ClosestTrav4<kWfShared, COUNT> tr;
+        bool active = false;
+        if (valid) {
+            const float4 o = A.ray_o[slot], d = A.ray_d[slot];
+            if (COUNT) rc.ext++;
+            active = !tr.init(S, Ray{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)}, 1e-4f, 1e9f, &rc.tc);
+        }
+        if (__any_sync(0xffffffffu, active)) {
+            int node = 0, sp = 0;
+            while (true) {
+                const WideNode w = load_wide(S.wide, node);
+                if (COUNT && active) rc.tc.nodes++;
+                float ee[4];
+                unsigned m = active ? slab4(w, tr.rp, tr.tmin, tr.t_best, ee) : 0u;
+                const unsigned lm = m & leaf_bits(w.ref);
+                m &= ~lm;
+                unsigned ulm = __reduce_or_sync(0xffffffffu, lm);
+                while (ulm) {
+                    const int k = __ffs(ulm) - 1;
+                    ulm &= ulm - 1;
+                    if (((lm >> k) & 1u) && pick_e(ee, k) <= tr.t_best)
+                        tr.test_leaf(S, pick_ref(w.ref, k), &rc.tc);
+                }
+                // per child, the smallest entry distance of a lane that still
+                // reaches it (entries are positive: their bits order as ints)
+                float key[4];
+                int ref[4] = {w.ref.x, w.ref.y, w.ref.z, w.ref.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const bool reach = ((m >> k) & 1u) && ee[k] <= tr.t_best;
+                    key[k] = __uint_as_float(__reduce_min_sync(
+                        0xffffffffu, reach ? __float_as_uint(ee[k]) : 0x7f800000u));
+                }
+                auto cs = [&](int a, int b) {
+                    if (key[b] < key[a]) {
+                        const float tk = key[a]; key[a] = key[b]; key[b] = tk;
+                        const int tr2 = ref[a]; ref[a] = ref[b]; ref[b] = tr2;
+                    }
+                };
+                cs(0, 1); cs(2, 3); cs(0, 2); cs(1, 3); cs(1, 2);
+                if (key[0] != INFINITY) {
+                    __syncwarp();
+                    if (lane == 0) {
+#pragma unroll
+                        for (int k = 3; k >= 1; --k)
+                            if (key[k] != INFINITY) { sref[sp] = ref[k]; skey[sp] = key[k]; ++sp; }
+                    } else {
+#pragma unroll
+                        for (int k = 3; k >= 1; --k)
+                            if (key[k] != INFINITY) ++sp;
+                    }
+                    __syncwarp();
+                    node = ref[0];
+                    continue;
+                }
+                // pop the nearest entry some lane may still reach
+                const float reach = __uint_as_float(__reduce_max_sync(
+                    0xffffffffu, active ? __float_as_uint(tr.t_best) : 0u));
+                bool found = false;
+                while (sp > 0) {
+                    --sp;
+                    if (skey[sp] <= reach) { node = sref[sp]; found = true; break; }
+                }
+                if (!found) break;
+            }
+        }
+        if (valid)
+            A.hit[slot] = make_float4(tr.t_best, __int_as_float(tr.best_ref),
+                                      __int_as_float(tr.best), 0.0f);
+    }
+    flush_counts<COUNT>(A, rc, 1);
 }
 
 // ---- shade --------------------------------------------------------------------
@@ -768,7 +869,7 @@ static int max_shadow_records(const SceneView& v, const std::vector<DevLight>& l
 }
 
 struct WfOccupancy {
-    int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_scatter = 0;
+    int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_scatter = 0, grid_packet = 0;
 };
 
 template <bool COUNT>
@@ -785,6 +886,10 @@ static cudaError_t occupancy(WfOccupancy& o) {
     o.grid_shade = sms * std::max(b2, 1);
     o.grid_shadow = sms * std::max(b3, 1);
     o.grid_scatter = sms * 8;
+    int b4 = 0;
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, wf_extend_packet<COUNT>, kWfBlock, 0);
+    o.grid_packet = sms * std::max(b4, 1);
     return e;
 }
 
@@ -822,6 +927,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
     WfOccupancy occ;
     cudaError_t e = occupancy<COUNT>(occ);
     if (e != cudaSuccess) return e;
+    const bool packet_first = jobs.size() == 1 && W.args.packets != 0;
     const WfArgs& A = W.args;
     const size_t smem = (size_t)kWfShared * kWfBlock * 8;
     // walk the path space in chunks of whole pixels
@@ -858,7 +964,10 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         n_launch += 1;
         for (int it = 0; it < iters; ++it) {
             lt.mark(KC_EXTEND, st, true);
-            wf_extend<COUNT><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
+            if (it == 0 && packet_first)
+                wf_extend_packet<COUNT><<<occ.grid_packet, kWfBlock, 0, st>>>(A);
+            else
+                wf_extend<COUNT><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
             lt.mark(KC_EXTEND, st, false);
             lt.mark(KC_SHADE, st, true);
             if (A.sort_key == 2) {
@@ -904,6 +1013,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     long long total_paths = 0;
     bool count = false;
     int qcap = 0, sort_key = 0, refill = 0;
+    bool packets = true;
     for (int k = 0; k < n; ++k) {
         const RenderCfg& c = cfgs[k];
         WfJob& J = jobs[k];
@@ -924,6 +1034,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
         if (c.queue_capacity > 0) qcap = c.queue_capacity;
         sort_key = c.sort_key;
         if (c.refill > 0) refill = c.refill;
+        packets = packets && c.packets;
     }
     total_paths = path_off;
     long long Q = qcap > 0 ? qcap : (1LL << 22);
@@ -935,6 +1046,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     W.args.n_jobs = n;
     W.args.counters = counters;
     W.args.sort_key = sort_key;
+    W.args.packets = packets ? 1 : 0;
     W.args.refill_below = refill > 0 ? refill : kDefaultRefill;
     W.args.maxS = maxS;
     if ((e = cudaMemcpyAsync(W.d_views, views.data(), views.size() * sizeof(SceneView),
@@ -951,6 +1063,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     mix((unsigned long long)Q);
     mix((unsigned long long)maxS);
     mix((unsigned long long)sort_key);
+    mix((unsigned long long)W.args.packets);
     mix((unsigned long long)W.args.refill_below);
     mix((unsigned long long)count);
     for (const auto& J : jobs) {

@@ -43,6 +43,7 @@ class RenderSettings:
     count_nodes: bool = False
     use_graph: bool = True
     profile_kernels: bool = False
+    packets: bool = True           # wavefront: camera rays traced as warp packets
     queue_capacity: int = 0
     sort_key: int = 0
     refill_below: int = 0
@@ -60,7 +61,8 @@ class RenderSettings:
         p.flags = ((A.FLAG_COUNT_RAYS if self.count_rays else 0) |
                    (A.FLAG_COUNT_NODES if self.count_nodes else 0) |
                    (0 if self.use_graph else A.FLAG_NO_GRAPH) |
-                   (A.FLAG_PROFILE_KERNELS if self.profile_kernels else 0))
+                   (A.FLAG_PROFILE_KERNELS if self.profile_kernels else 0) |
+                   (0 if self.packets else A.FLAG_NO_PACKETS))
         p.queue_capacity, p.sort_key = self.queue_capacity, self.sort_key
         p.refill_below = self.refill_below
         return p
