@@ -398,8 +398,8 @@ def _event_ms(stream, fn, reps: int) -> float:
 
 def measure_extras(ctx, sid, st, img, stream) -> dict:
     """Outside the timed region: image quality against a 4096-spp render of
-    the bench frame, the adjoint of the box configuration, and the batch of
-    256 uneven scenes."""
+    the bench frame, the adjoint of the box configuration, the batch of 256
+    uneven scenes and the triangle-mesh configuration."""
     import dataclasses
 
     import torch
@@ -471,7 +471,52 @@ def measure_extras(ctx, sid, st, img, stream) -> dict:
                     "one_by_one_megakernel_ms": mk_ms}
     for s_ in sids:
         ctx.free(s_)
+    out["mesh"] = measure_mesh(ctx, stream)
     return out
+
+
+def measure_mesh(ctx, stream) -> dict:
+    """The triangle-mesh configuration: a displaced icosphere (8
+    subdivisions, 1,310,720 triangles, float32 vertices, int32 indices) in a
+    box lit by a 0.25 x 0.25 emissive ceiling quad with next-event
+    estimation; 1024x1024, 64 spp, depth 12 (67,108,864 paths per frame)."""
+    import time
+
+    import torch
+    from pencil_b200 import _abi as A
+    from pencil_b200 import workloads as W
+    from pencil_b200.renderer import RenderStats
+    wm = W.mesh_box()
+    nodes, depth = wm.scene.build_bvh()       # Pencil builds its tree at parse time
+    t0 = time.perf_counter()
+    sm = ctx.upload(wm.scene, nodes)
+    upload_ms = (time.perf_counter() - t0) * 1e3
+    info = ctx.scene_info(sm)
+    st = wm.settings
+    st.queue_capacity, st.refill_below, st.sort_key = 1 << 24, 16, 2
+    paths = st.width * st.height * st.samples ** 2
+    buf = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")
+    st.engine = A.ENGINE_WAVEFRONT
+    wf_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 2)
+    cnt = RenderStats()
+    st.count_rays = True
+    ctx.render(sm, st, stats=cnt)
+    st.count_rays = False
+    st.engine = A.ENGINE_MEGAKERNEL
+    mk_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 1)
+    ctx.free(sm)
+    rays = cnt.extension_rays + cnt.shadow_rays
+    return {"workload": "mesh_box: displaced icosphere 1,310,720 triangles in a box, quad-light "
+                        "NEE, 1024x1024, 64 spp, depth 12",
+            "paths": paths, "triangles": int(len(wm.scene.mesh_indices)),
+            "bvh_depth": int(depth), "wide_nodes": info["n_wide"],
+            "device_bytes": info["device_bytes"], "upload_ms": upload_ms,
+            "wavefront_ms": wf_ms, "wavefront_mpaths_s": paths / wf_ms / 1e3,
+            "wavefront_mrays_s": rays / wf_ms / 1e3,
+            "megakernel_ms": mk_ms, "megakernel_mpaths_s": paths / mk_ms / 1e3,
+            "wavefront_over_megakernel": mk_ms / wf_ms,
+            "settings": {"queue_capacity": st.queue_capacity, "refill_below": st.refill_below,
+                         "sort_key": st.sort_key}}
 
 
 class _Null:

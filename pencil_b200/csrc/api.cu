@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -12,6 +13,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "host_internal.h"
@@ -129,6 +131,13 @@ struct pgpu_ctx {
     size_t stage_cap = 0;
     unsigned char* d_adj = nullptr;   // adjoint inputs and gradient sums
     size_t adj_cap = 0;
+    // scene arenas come from a stream-ordered pool owned by the context, so
+    // that upload / free cycles reuse device memory without cudaMalloc or
+    // cudaFree (each of which synchronises the device)
+    cudaMemPool_t pool = nullptr;
+    // host workspace of uploads, kept between calls (no page faults on reuse)
+    std::vector<int> ws_idx, ws_leaf_ref;
+    std::vector<float4> ws_wide;
 };
 
 namespace {
@@ -147,6 +156,55 @@ int fail(pgpu_ctx* c, int code, const char* fmt, ...) {
 
 int cuda_fail(pgpu_ctx* c, cudaError_t e, const char* what) {
     return fail(c, PGPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// f(begin, end) over [0, n) on up to 16 host threads (one when n is small).
+template <class F>
+void parallel_for(int n, F f) {
+    constexpr int kGrain = 16384;
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int T = std::min({16, hw, (n + kGrain - 1) / kGrain});
+    if (T <= 1) { f(0, n); return; }
+    std::vector<std::thread> th;
+    th.reserve(T - 1);
+    const int chunk = (n + T - 1) / T;
+    for (int t = 1; t < T; ++t) {
+        const int b = t * chunk, e = std::min(n, b + chunk);
+        if (b < e) th.emplace_back([=] { f(b, e); });
+    }
+    f(0, std::min(n, chunk));
+    for (auto& x : th) x.join();
+}
+
+// Smallest index in [0, n) for which bad(k) holds, or -1 (threads).
+template <class P>
+int first_bad(int n, P bad) {
+    std::atomic<int> first{n};
+    parallel_for(n, [&](int b, int e) {
+        for (int k = b; k < e && k < first.load(std::memory_order_relaxed); ++k)
+            if (bad(k)) {
+                int cur = first.load();
+                while (k < cur && !first.compare_exchange_weak(cur, k)) {}
+                break;
+            }
+    });
+    return first.load() < n ? first.load() : -1;
+}
+
+// Scene arena from the context's memory pool (created on first use).
+cudaError_t arena_alloc(pgpu_ctx* c, size_t bytes, void** out) {
+    if (!c->pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = c->device;
+        cudaError_t e = cudaMemPoolCreate(&c->pool, &props);
+        if (e != cudaSuccess) { c->pool = nullptr; return e; }
+        // keep freed arenas for the next upload (released with the context)
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    return cudaMallocFromPoolAsync(out, bytes, c->pool, c->stream);
 }
 
 #define PGPU_CUDA(ctx, call)                                          \
@@ -187,37 +245,40 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     if (n_nodes != 2 * n_prims - 1)
         return fail(c, PGPU_ERR_BVH_INVALID, "%d nodes for %d primitives (need 2n-1)", n_nodes,
                     n_prims);
-    std::vector<char> seen_prim(n_prims, 0);
-    std::vector<std::pair<int, int>> st;   // node, level
-    st.push_back({0, 1});
-    int visited = 0;
-    while (!st.empty()) {
-        auto [k, lvl] = st.back();
-        st.pop_back();
-        if (k < 0 || k >= n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "node index %d out of range", k);
-        // popping left before right visits nodes in pre-order: the table must
-        // list them in exactly that order
-        if (k != visited)
-            return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
-        ++visited;
-        depth = std::max(depth, lvl);
+    // DFS pre-order (the order Pencil's recursive build emits): an interior
+    // node k has its left subtree at k + 1 and its right subtree right after
+    // the left one. Subtree sizes, from the back, check exactly that.
+    std::vector<int> size(n_nodes);
+    for (int k = n_nodes - 1; k >= 0; --k) {
         const pgpu_bvh_node& nd = nodes[k];
         if (!finite3(nd.bmin) || !finite3(nd.bmax))
             return fail(c, PGPU_ERR_BVH_INVALID, "node %d has a non-finite box", k);
         if (nd.left < 0) {
             if (nd.right < 0 || nd.right >= n_prims)
                 return fail(c, PGPU_ERR_BVH_INVALID, "leaf %d references primitive %d", k, nd.right);
+            size[k] = 1;
+            continue;
+        }
+        if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes ||
+            nd.right != nd.left + size[nd.left])
+            return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
+        size[k] = 1 + size[nd.left] + size[nd.right];
+    }
+    if (size[0] != n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "unreachable nodes in table");
+    // every primitive in exactly one leaf; levels
+    std::vector<int> level(n_nodes);
+    std::vector<char> seen_prim(n_prims, 0);
+    level[0] = 1;
+    for (int k = 0; k < n_nodes; ++k) {
+        const pgpu_bvh_node& nd = nodes[k];
+        depth = std::max(depth, level[k]);
+        if (nd.left < 0) {
             if (seen_prim[nd.right]++)
                 return fail(c, PGPU_ERR_BVH_INVALID, "primitive %d is in two leaves", nd.right);
         } else {
-            if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes)
-                return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
-            st.push_back({nd.right, lvl + 1});
-            st.push_back({nd.left, lvl + 1});
+            level[nd.left] = level[nd.right] = level[k] + 1;
         }
-        if (visited > n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "node table has a cycle");
     }
-    if (visited != n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "unreachable nodes in table");
     if (depth > kMaxDepth)
         return fail(c, PGPU_ERR_UNSUPPORTED, "BVH depth %d exceeds %d", depth, kMaxDepth);
     return PGPU_OK;
@@ -269,8 +330,10 @@ void pgpu_destroy(pgpu_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (auto& kv : c->scenes) cudaFree(kv.second->arena);
+    for (auto& kv : c->scenes) cudaFreeAsync(kv.second->arena, c->stream);
     c->scenes.clear();
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->pool) cudaMemPoolDestroy(c->pool);
     cudaFree(c->d_out);
     cudaFree(c->d_m2);
     cudaFree(c->d_cnt);
@@ -336,9 +399,16 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     const long long n_unified = (long long)s->n_prims + s->n_mesh_triangles;
     if (n_unified >= kMaxLeaves) return fail(c, PGPU_ERR_UNSUPPORTED, "too many primitives");
     const int nU = (int)n_unified;
-    for (int k = 0; k < s->n_prims; ++k) {
-        int rc = check_prim(c, s->prims[k], k, s->n_materials);
-        if (rc) return rc;
+    {
+        const int bad = first_bad(s->n_prims, [&](int k) {
+            const pgpu_prim& p = s->prims[k];
+            if (p.type < PGPU_PRIM_SPHERE || p.type > PGPU_PRIM_CONE) return true;
+            if (p.material < 0 || p.material >= s->n_materials) return true;
+            for (int q = 0; q < 14; ++q)
+                if (!std::isfinite(p.p[q])) return true;
+            return false;
+        });
+        if (bad >= 0) return check_prim(c, s->prims[bad], bad, s->n_materials);
     }
     for (int k = 0; k < s->n_mesh_triangles; ++k) {
         for (int v = 0; v < 3; ++v) {
@@ -352,23 +422,33 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     for (int k = 0; k < s->n_mesh_vertices; ++k)
         if (!finite3(s->mesh_vertices + 3 * k))
             return fail(c, PGPU_ERR_INVALID_ARG, "mesh vertex %d is not finite", k);
-    std::vector<DevMaterial> mats(s->n_materials);
-    for (int k = 0; k < s->n_materials; ++k) {
-        const pgpu_material& m = s->materials[k];
-        if (m.kind < PGPU_MAT_DIFFUSE || m.kind > PGPU_MAT_DIELECTRIC)
-            return fail(c, PGPU_ERR_UNSUPPORTED, "material %d has unsupported kind %d", k, m.kind);
-        if (m.flags != 0) return fail(c, PGPU_ERR_UNSUPPORTED, "material %d has flags set", k);
-        DevMaterial d{};
-        std::memcpy(d.albedo, m.albedo, 12);
-        d.kind = m.kind;
-        std::memcpy(d.emission, m.emission, 12);
-        d.reflectivity = m.reflectivity;
-        d.ior = m.ior;
-        d.specular = m.specular;
-        d.shininess = m.shininess;
-        std::memcpy(d.specular_color, m.specular_color, 12);
-        mats[k] = d;
+    {
+        const int bad = first_bad(s->n_materials, [&](int k) {
+            const pgpu_material& m = s->materials[k];
+            return m.kind < PGPU_MAT_DIFFUSE || m.kind > PGPU_MAT_DIELECTRIC || m.flags != 0;
+        });
+        if (bad >= 0) {
+            const pgpu_material& m = s->materials[bad];
+            if (m.flags != 0) return fail(c, PGPU_ERR_UNSUPPORTED, "material %d has flags set", bad);
+            return fail(c, PGPU_ERR_UNSUPPORTED, "material %d has unsupported kind %d", bad, m.kind);
+        }
     }
+    std::vector<DevMaterial> mats(s->n_materials);
+    parallel_for(s->n_materials, [&](int b, int e) {
+        for (int k = b; k < e; ++k) {
+            const pgpu_material& m = s->materials[k];
+            DevMaterial d{};
+            std::memcpy(d.albedo, m.albedo, 12);
+            d.kind = m.kind;
+            std::memcpy(d.emission, m.emission, 12);
+            d.reflectivity = m.reflectivity;
+            d.ior = m.ior;
+            d.specular = m.specular;
+            d.shininess = m.shininess;
+            std::memcpy(d.specular_color, m.specular_color, 12);
+            mats[k] = d;
+        }
+    });
     std::vector<DevLight> lights(s->n_lights);
     std::vector<int> quad_mats;
     int has_quad = 0;
@@ -398,13 +478,13 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     }
 
     // BVH: caller's table (Pencil's tree) or the same tree built here
-    std::vector<pgpu_prim> prims;
-    unified_prims(*s, prims);
     std::vector<pgpu_bvh_node> built;
     const pgpu_bvh_node* nodes = s->nodes;
     int n_nodes = s->n_nodes;
     int depth = 0;
     if (!nodes) {
+        std::vector<pgpu_prim> prims;
+        unified_prims(*s, prims);
         build_bvh(prims, built, depth);
         nodes = built.data();
         n_nodes = (int)built.size();
@@ -413,7 +493,8 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     if (rc) return rc;
 
     // DFS order numbering: interior nodes and leaf slots
-    std::vector<int> idx(n_nodes);
+    std::vector<int>& idx = c->ws_idx;
+    idx.resize(n_nodes);
     int n_int = 0, n_leaf = 0;
     for (int k = 0; k < n_nodes; ++k) idx[k] = nodes[k].left < 0 ? n_leaf++ : n_int++;
     // vertices: mesh vertices first, then those of explicit triangles
@@ -428,10 +509,12 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         return ~((type << kLeafTypeShift) | idx[k]);
     };
     // 4-wide nodes for the wavefront's traversal
-    std::vector<int> leaf_ref(n_nodes, 0);
-    for (int k = 0; k < n_nodes; ++k)
-        if (nodes[k].left < 0) leaf_ref[k] = ref_of(k);
-    std::vector<float4> wide;
+    std::vector<int>& leaf_ref = c->ws_leaf_ref;
+    leaf_ref.resize(n_nodes);
+    parallel_for(n_nodes, [&](int b, int e) {
+        for (int k = b; k < e; ++k) leaf_ref[k] = nodes[k].left < 0 ? ref_of(k) : 0;
+    });
+    std::vector<float4>& wide = c->ws_wide;
     int wide_stack = 0;
     const int n_wide = collapse_wide(nodes, n_nodes, leaf_ref, kMaxDepth, wide, wide_stack);
     if (wide_stack > kMaxDepth)
@@ -459,7 +542,21 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         c->stage_cap = total;
     }
     unsigned char* host = c->h_stage;
-    std::memset(host, 0, total);
+    // every byte is written below except geo_b of one-word primitives and the
+    // alignment gaps; those are zeroed so that uploads are deterministic
+    {
+        const size_t ends[][2] = {{off_nodes + (size_t)n_int * 64, off_wide},
+                                  {off_wide + (size_t)n_wide * kWideNodeFloat4 * 16, off_ga},
+                                  {off_ga + (size_t)n_leaf * 16, off_gb},
+                                  {off_gb, off_vt},
+                                  {off_vt + n_verts * 16, off_lm},
+                                  {off_lm + (size_t)n_leaf * 4, off_lp},
+                                  {off_lp + (size_t)n_leaf * 4, off_mt},
+                                  {off_mt + mats.size() * sizeof(DevMaterial), off_lt},
+                                  {off_lt + lights.size() * sizeof(DevLight), total}};
+        for (const auto& g : ends)
+            if (g[1] > g[0]) std::memset(host + g[0], 0, g[1] - g[0]);
+    }
     float4* h_nodes = reinterpret_cast<float4*>(host + off_nodes);
     float4* h_ga = reinterpret_cast<float4*>(host + off_ga);
     float4* h_gb = reinterpret_cast<float4*>(host + off_gb);
@@ -470,8 +567,10 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         h_vt[k] = make_float4(s->mesh_vertices[3 * k], s->mesh_vertices[3 * k + 1],
                               s->mesh_vertices[3 * k + 2], 0.0f);
     size_t next_vert = (size_t)s->n_mesh_vertices;
-    if (n_wide) std::memcpy(host + off_wide, wide.data(), wide.size() * sizeof(float4));
-    for (int k = 0; k < n_nodes; ++k) {
+    if (n_wide) std::memcpy(host + off_wide, wide.data(), (size_t)n_wide * kWideNodeFloat4 * 16);
+    // explicit triangles take vertices in DFS leaf order: sequential then
+    auto convert = [&](int kb, int ke) {
+    for (int k = kb; k < ke; ++k) {
         const pgpu_bvh_node& nd = nodes[k];
         if (nd.left >= 0) {
             const pgpu_bvh_node& L = nodes[nd.left];
@@ -522,12 +621,15 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
                 break;
         }
     }
+    };
+    if (n_explicit_tri > 0) convert(0, n_nodes);
+    else parallel_for(n_nodes, convert);
     std::memcpy(host + off_mt, mats.data(), mats.size() * sizeof(DevMaterial));
     std::memcpy(host + off_lt, lights.data(), lights.size() * sizeof(DevLight));
 
     PGPU_CUDA(c, cudaSetDevice(c->device));
     auto ds = std::make_unique<DeviceScene>();
-    cudaError_t e = cudaMalloc(&ds->arena, total);
+    cudaError_t e = arena_alloc(c, total, &ds->arena);
     if (e != cudaSuccess)
         return fail(c, PGPU_ERR_OUT_OF_MEMORY, "scene arena of %zu bytes: %s", total,
                     cudaGetErrorString(e));
@@ -535,7 +637,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     e = cudaMemcpyAsync(ds->arena, host, total, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
-        cudaFree(ds->arena);
+        cudaFreeAsync(ds->arena, c->stream);
         return cuda_fail(c, e, "scene upload");
     }
     unsigned char* base = static_cast<unsigned char*>(ds->arena);
@@ -568,9 +670,9 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     ds->n_wide = n_wide;
     ds->wide_stack = wide_stack;
     ds->depth = depth;
-    ds->mats = mats;
-    ds->lights = lights;
-    ds->quad_mats = quad_mats;
+    ds->mats = std::move(mats);
+    ds->lights = std::move(lights);
+    ds->quad_mats = std::move(quad_mats);
     ds->d_mats = reinterpret_cast<DevMaterial*>(base + off_mt);
     int id = c->next_id++;
     c->scenes[id] = std::move(ds);
@@ -582,8 +684,10 @@ int32_t pgpu_free_scene(pgpu_ctx* c, int32_t id) {
     if (!c) return PGPU_ERR_INVALID_ARG;
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
+    // work on the context stream that reads the scene finishes first; the
+    // arena then returns to the pool
     cudaStreamSynchronize(c->stream);
-    cudaFree(ds->arena);
+    cudaFreeAsync(ds->arena, c->stream);
     c->scenes.erase(id);
     return PGPU_OK;
 }

@@ -42,7 +42,6 @@ struct Collapser {
     // the stack entries a traversal below it can hold (`need`).
     int build(int b, int& need) {
         const int w = n_wide++;
-        out.resize((size_t)n_wide * kWideNodeFloat4);
         int ch[4] = {nodes[b].left, nodes[b].right, -1, -1};
         int n = 2;
         while (expand && n < 4) {
@@ -100,14 +99,18 @@ struct Collapser {
 
 int collapse_wide(const pgpu_bvh_node* nodes, int n_nodes, const std::vector<int>& leaf_ref,
                   int max_stack, std::vector<float4>& out, int& stack_need) {
-    out.clear();
     stack_need = 0;
     if (n_nodes == 0 || nodes[0].left < 0) return 0;
     // greedy collapse; if a pathological tree would need a deeper stack than
     // the kernels hold, two children per node (the binary tree's own bound)
     int n_wide = 0;
+    int n_interior = 0;
+    for (int k = 0; k < n_nodes; ++k) n_interior += nodes[k].left >= 0;
+    // at most one wide node per binary interior node; `out` only grows, so a
+    // reused vector is neither reallocated nor cleared
+    if (out.size() < (size_t)n_interior * kWideNodeFloat4)
+        out.resize((size_t)n_interior * kWideNodeFloat4);
     for (int pass = 0; pass < 2; ++pass) {
-        out.clear();
         Collapser c{nodes, leaf_ref, pass == 0, out};
         int need = 0;
         c.build(0, need);

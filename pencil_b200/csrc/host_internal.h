@@ -18,8 +18,9 @@ int make_prim(int type, int material, const float* a, const float* b, const floa
               float s1, pgpu_prim* out);
 
 // bvh_wide.cpp: 4-wide nodes (kWideNodeFloat4 float4 each) collapsed from a
-// validated binary tree in DFS pre-order. leaf_ref[k] is the leaf ref of
-// binary leaf k. Returns the number of wide nodes (0 when the root is a
+// validated binary tree in DFS pre-order, written to the front of `out`
+// (which grows as needed and is never shrunk). leaf_ref[k] is the leaf ref
+// of binary leaf k. Returns the number of wide nodes (0 when the root is a
 // leaf); stack_need receives the most stack entries a traversal holds, which
 // is at most max_stack unless the binary tree itself needs more.
 int collapse_wide(const pgpu_bvh_node* nodes, int n_nodes, const std::vector<int>& leaf_ref,
