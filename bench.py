@@ -63,6 +63,9 @@ def parse_args():
                     help="render the workload once, kernels launched one by one (for ncu)")
     ap.add_argument("--profile-scale", type=int, default=1,
                     help="divide the image width and height by this (smaller ncu cases)")
+    ap.add_argument("--profile-counts", action="store_true",
+                    help="with --profile-case: also render once with ray counters and "
+                         "print them (run without ncu)")
     return ap.parse_args()
 
 
@@ -201,9 +204,10 @@ def run_ours(args) -> None:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    from pencil_b200.distributed import combine, shard_settings
     wl = W.sphere_cloud()
-    st: RenderSettings = wl.settings
-    st.sample_offset = rank * st.samples * st.samples
+    # every rank renders the whole frame with its own samples (weak scaling)
+    st: RenderSettings = shard_settings(wl.settings, rank, world)
     paths_per_frame = st.width * st.height * st.samples ** 2
     ctx = GpuContext(local)
     stream = torch.cuda.ExternalStream(ctx.stream)
@@ -229,9 +233,8 @@ def run_ours(args) -> None:
         st.engine = engine
         for _ in range(warmup):
             ctx.render_device(sid, st, img.data_ptr())
-            if world > 1:
-                with torch.cuda.stream(stream):
-                    dist.all_reduce(img)
+            with torch.cuda.stream(stream):
+                combine(img, world)
         evs = []
         barrier()
         cm = clocks if clocks is not None else _Null()
@@ -243,9 +246,8 @@ def run_ours(args) -> None:
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
                 ctx.render_device(sid, st, img.data_ptr())
-                if world > 1:
-                    with torch.cuda.stream(stream):
-                        dist.all_reduce(img)
+                with torch.cuda.stream(stream):
+                    combine(img, world)        # the frame's one exchange
                 e1.record(stream)
                 evs.append((e0, e1))
             barrier()
@@ -537,15 +539,25 @@ def run_profile_case(args) -> None:
     st.width //= args.profile_scale
     st.height //= args.profile_scale
     st.use_graph = False
-    st.queue_capacity, st.refill_below = 1 << 22, 16
+    # the launch parameters the autotuner picks for this workload: one chunk,
+    # refill at 16 busy lanes, shadow work sorted by origin cell
+    st.queue_capacity = st.width * st.height * st.samples ** 2
+    st.refill_below, st.sort_key = 16, 2
     st.engine = A.ENGINE_WAVEFRONT if args.profile_case == "wavefront" else A.ENGINE_MEGAKERNEL
     ctx = GpuContext(0)
     sid = ctx.upload(wl.scene)
     stats = RenderStats()
     img = ctx.render(sid, st, stats=stats)
     assert np.isfinite(img).all()
-    print(json.dumps({"profile_case": args.profile_case, "width": st.width, "height": st.height,
-                      "launches": stats.kernel_launches, "device_ms": stats.device_ms}))
+    out = {"profile_case": args.profile_case, "width": st.width, "height": st.height,
+           "launches": stats.kernel_launches, "device_ms": stats.device_ms}
+    if args.profile_counts:
+        cnt = RenderStats()
+        st.count_rays, st.count_nodes = True, True
+        ctx.render(sid, st, stats=cnt)
+        out.update(extension_rays=cnt.extension_rays, shadow_rays=cnt.shadow_rays,
+                   ext_node_visits=cnt.ext_node_visits, shadow_node_visits=cnt.shadow_node_visits)
+    print(json.dumps(out))
     ctx.free(sid)
     ctx.close()
 
