@@ -138,6 +138,7 @@ struct pgpu_ctx {
     // host workspace of uploads, kept between calls (no page faults on reuse)
     std::vector<int> ws_idx, ws_leaf_ref;
     std::vector<float4> ws_wide;
+    std::vector<DevMaterial> spare_mats;   // material table of the last freed scene
 };
 
 namespace {
@@ -433,7 +434,9 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
             return fail(c, PGPU_ERR_UNSUPPORTED, "material %d has unsupported kind %d", bad, m.kind);
         }
     }
-    std::vector<DevMaterial> mats(s->n_materials);
+    std::vector<DevMaterial> mats = std::move(c->spare_mats);   // pages already mapped
+    c->spare_mats = {};
+    mats.resize(s->n_materials);
     parallel_for(s->n_materials, [&](int b, int e) {
         for (int k = b; k < e; ++k) {
             const pgpu_material& m = s->materials[k];
@@ -688,6 +691,7 @@ int32_t pgpu_free_scene(pgpu_ctx* c, int32_t id) {
     // arena then returns to the pool
     cudaStreamSynchronize(c->stream);
     cudaFreeAsync(ds->arena, c->stream);
+    if (ds->mats.capacity() > c->spare_mats.capacity()) c->spare_mats.swap(ds->mats);
     c->scenes.erase(id);
     return PGPU_OK;
 }

@@ -16,6 +16,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include <vector_functions.h>
@@ -31,6 +33,44 @@ float area(const pgpu_bvh_node& n) {
     return 2.0f * (dx * dy + dy * dz + dz * dx);
 }
 
+void write_node(float4* q, const float (&lo)[3][4], const float (&hi)[3][4], const int (&ref)[4]) {
+    q[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    q[1] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    q[2] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    q[3] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    q[4] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    q[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    static_assert(sizeof(ref) == sizeof(float4), "four refs fill one float4");
+    std::memcpy(&q[6], ref, sizeof(ref));
+    q[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// Copies each subtree's block into `out` at base[t], its interior refs
+// (local indices) shifted by base[t].
+void parallel_relocate(std::vector<float4>& out, const std::vector<std::vector<float4>>& local,
+                       const std::vector<int>& count, const std::vector<int>& base) {
+    const int n = (int)local.size();
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int T = std::max(1, std::min({16, hw, n}));
+    std::atomic<int> next{0};
+    auto worker = [&] {
+        for (int t; (t = next.fetch_add(1)) < n;) {
+            const int cnt = count[t];
+            float4* dst = out.data() + (size_t)base[t] * kWideNodeFloat4;
+            std::copy_n(local[t].begin(), (size_t)cnt * kWideNodeFloat4, dst);
+            for (int w = 0; w < cnt; ++w) {
+                int* refs = reinterpret_cast<int*>(dst + (size_t)w * kWideNodeFloat4 + 6);
+                for (int k = 0; k < 4; ++k)
+                    if (refs[k] >= 0) refs[k] += base[t];
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    for (int k = 1; k < T; ++k) th.emplace_back(worker);
+    worker();
+    for (auto& x : th) x.join();
+}
+
 struct Collapser {
     const pgpu_bvh_node* nodes;
     const std::vector<int>& leaf_ref;
@@ -42,6 +82,8 @@ struct Collapser {
     // the stack entries a traversal below it can hold (`need`).
     int build(int b, int& need) {
         const int w = n_wide++;
+        if (out.size() < (size_t)n_wide * kWideNodeFloat4)
+            out.resize(std::max(out.size() * 2, (size_t)n_wide * kWideNodeFloat4));
         int ch[4] = {nodes[b].left, nodes[b].right, -1, -1};
         int n = 2;
         while (expand && n < 4) {
@@ -81,19 +123,117 @@ struct Collapser {
         }
         // a step pushes every interior child it enters but the nearest
         need = std::max(0, interior - 1) + deepest;
-        float4* q = out.data() + (size_t)w * kWideNodeFloat4;
-        q[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
-        q[1] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
-        q[2] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
-        q[3] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
-        q[4] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
-        q[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
-        static_assert(sizeof(ref) == sizeof(float4), "four refs fill one float4");
-        std::memcpy(&q[6], ref, sizeof(ref));
-        q[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        write_node(out.data() + (size_t)w * kWideNodeFloat4, lo, hi, ref);
         return w;
     }
 };
+
+// The top of the tree is collapsed on this thread until there are enough
+// independent subtrees; each subtree is then collapsed on its own thread into
+// a local array and appended. Wide nodes need no particular numbering (the
+// kernels only follow refs), so the top comes first and each subtree's nodes
+// follow as one block in DFS pre-order.
+int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_ref,
+                      bool expand, int threads, std::vector<float4>& out, int& stack_need) {
+    const int T = threads;
+    // top: breadth-first over wide-node roots until enough subtrees wait
+    struct Pending { int binary; int parent; int child; };   // ref slot to patch
+    std::vector<Pending> todo{{0, -1, -1}};
+    std::vector<float4> top;
+    size_t head = 0;
+    const size_t want = T > 1 ? (size_t)T * 8 : 0;
+    std::vector<std::vector<int>> top_kids;  // per top node: its subtrees' todo indices
+    int n_top = 0;
+    while (head < todo.size() && todo.size() - head < want) {
+        const Pending p = todo[head++];
+        // collapse one node without recursing into interior children
+        int ch[4] = {nodes[p.binary].left, nodes[p.binary].right, -1, -1};
+        int n = 2;
+        while (expand && n < 4) {
+            int pick = -1;
+            float best = -1.0f;
+            for (int k = 0; k < n; ++k) {
+                const pgpu_bvh_node& c = nodes[ch[k]];
+                if (c.left >= 0 && area(c) > best) { best = area(c); pick = k; }
+            }
+            if (pick < 0) break;
+            const int l = nodes[ch[pick]].left, r = nodes[ch[pick]].right;
+            for (int k = n; k > pick + 1; --k) ch[k] = ch[k - 1];
+            ch[pick] = l;
+            ch[pick + 1] = r;
+            ++n;
+        }
+        const int w = n_top++;
+        top.resize((size_t)n_top * kWideNodeFloat4);
+        top_kids.emplace_back();
+        float lo[3][4], hi[3][4];
+        int ref[4];
+        for (int k = 0; k < 4; ++k) {
+            if (k >= n) {
+                for (int a = 0; a < 3; ++a) { lo[a][k] = INFINITY; hi[a][k] = -INFINITY; }
+                ref[k] = ~(kLeafNone << kLeafTypeShift);
+                continue;
+            }
+            const pgpu_bvh_node& c = nodes[ch[k]];
+            for (int a = 0; a < 3; ++a) { lo[a][k] = c.bmin[a]; hi[a][k] = c.bmax[a]; }
+            if (c.left < 0) {
+                ref[k] = leaf_ref[ch[k]];
+            } else {
+                ref[k] = -1;                 // patched below
+                top_kids.back().push_back((int)todo.size());
+                todo.push_back({ch[k], w, k});
+            }
+        }
+        write_node(top.data() + (size_t)w * kWideNodeFloat4, lo, hi, ref);
+    }
+    // remaining subtrees in parallel
+    const int n_tasks = (int)(todo.size() - head);
+    std::vector<std::vector<float4>> local(n_tasks);
+    std::vector<int> local_n(n_tasks, 0), local_need(n_tasks, 0);
+    auto run = [&](int t) {
+        Collapser c{nodes, leaf_ref, expand, local[t]};
+        local[t].reserve(1024);
+        c.build(todo[head + t].binary, local_need[t]);
+        local_n[t] = c.n_wide;
+    };
+    {
+        std::vector<std::thread> th;
+        std::atomic<int> next{0};
+        auto worker = [&] { for (int t; (t = next.fetch_add(1)) < n_tasks;) run(t); };
+        const int nt = std::min(T, std::max(1, n_tasks));
+        for (int k = 1; k < nt; ++k) th.emplace_back(worker);
+        worker();
+        for (auto& x : th) x.join();
+    }
+    // layout: top nodes, then each task's block
+    std::vector<int> base(n_tasks);
+    int total = n_top;
+    for (int t = 0; t < n_tasks; ++t) { base[t] = total; total += local_n[t]; }
+    if (out.size() < (size_t)total * kWideNodeFloat4) out.resize((size_t)total * kWideNodeFloat4);
+    std::copy(top.begin(), top.end(), out.begin());
+    // which todo entry is which task: entries [head, end) are tasks; entries
+    // before head became top nodes 0, 1, ... in order
+    std::vector<int> wide_of_todo(todo.size());
+    for (size_t k = 0; k < head; ++k) wide_of_todo[k] = (int)k;
+    for (int t = 0; t < n_tasks; ++t) wide_of_todo[head + t] = base[t];
+    for (size_t k = 1; k < todo.size(); ++k) {
+        const Pending& p = todo[k];
+        int* refs = reinterpret_cast<int*>(out.data() + (size_t)p.parent * kWideNodeFloat4 + 6);
+        refs[p.child] = wide_of_todo[k];
+    }
+    parallel_relocate(out, local, local_n, base);
+    // stack need: tasks' own, then the top nodes bottom-up (children of a top
+    // node come later in todo, so a reverse sweep sees them first)
+    std::vector<int> need_of_todo(todo.size(), 0);
+    for (int t = 0; t < n_tasks; ++t) need_of_todo[head + t] = local_need[t];
+    for (int w = n_top - 1; w >= 0; --w) {
+        int interior = 0, deepest = 0;
+        for (int k : top_kids[w]) { ++interior; deepest = std::max(deepest, need_of_todo[k]); }
+        need_of_todo[w] = std::max(0, interior - 1) + deepest;
+    }
+    stack_need = need_of_todo[0];
+    return total;
+}
 
 }  // namespace
 
@@ -101,22 +241,21 @@ int collapse_wide(const pgpu_bvh_node* nodes, int n_nodes, const std::vector<int
                   int max_stack, std::vector<float4>& out, int& stack_need) {
     stack_need = 0;
     if (n_nodes == 0 || nodes[0].left < 0) return 0;
-    // greedy collapse; if a pathological tree would need a deeper stack than
-    // the kernels hold, two children per node (the binary tree's own bound)
-    int n_wide = 0;
     int n_interior = 0;
     for (int k = 0; k < n_nodes; ++k) n_interior += nodes[k].left >= 0;
     // at most one wide node per binary interior node; `out` only grows, so a
     // reused vector is neither reallocated nor cleared
     if (out.size() < (size_t)n_interior * kWideNodeFloat4)
         out.resize((size_t)n_interior * kWideNodeFloat4);
+    // greedy collapse; if a pathological tree would need a deeper stack than
+    // the kernels hold, two children per node (the binary tree's own bound)
+    // threads only pay off for large trees
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int threads = n_interior < 16384 ? 1 : std::min(16, hw);
+    int n_wide = 0;
     for (int pass = 0; pass < 2; ++pass) {
-        Collapser c{nodes, leaf_ref, pass == 0, out};
-        int need = 0;
-        c.build(0, need);
-        stack_need = need;
-        n_wide = c.n_wide;
-        if (need <= max_stack) break;
+        n_wide = collapse_parallel(nodes, leaf_ref, pass == 0, threads, out, stack_need);
+        if (stack_need <= max_stack) break;
     }
     return n_wide;
 }
