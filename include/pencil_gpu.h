@@ -209,8 +209,11 @@ enum pgpu_flags {
                                      instead of replaying a CUDA graph       */
     PGPU_FLAG_PROFILE_KERNELS = 16, /* time each kernel class (implies
                                      NO_GRAPH); see pgpu_stats.kernel_ms     */
-    PGPU_FLAG_NO_PACKETS    = 32  /* wavefront: trace camera rays one per lane
+    PGPU_FLAG_NO_PACKETS    = 32, /* wavefront: trace camera rays one per lane
                                      instead of as warp packets              */
+    PGPU_FLAG_MIS           = 64  /* path tracing with trace_path_mis's light
+                                     weights (RenderSettings::mis,
+                                     src/renderer.hpp:55, 1205-1346)         */
 };
 
 typedef struct pgpu_render_params {

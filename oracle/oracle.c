@@ -524,6 +524,32 @@ static v3 whitted(ctx_t* c, ray_t r, int depth, rng_t* rng) {
     return local;
 }
 
+/* Contribution of a visible point/directional light sample at a path-trace
+ * vertex: trace_path (src/renderer.hpp:912-913) or, with PGPU_FLAG_MIS,
+ * trace_path_mis (src/renderer.hpp:1264-1297): the power heuristic of the
+ * light pdf (a disc light's, for a light facing down, cosine >= 0.01) and the
+ * cosine BSDF pdf, mixing albedo*I*(n.L) and albedo*I; nothing when n.L <= 0. */
+static v3 light_term(const pgpu_light* l, int mis, v3 T, v3 albedo, v3 L, float dist,
+                     float ndotl) {
+    if (!mis) return mulf(mulv(mulv(T, albedo), ld3(l->intensity)), ndotl);
+    if (ndotl <= 0.0f) return mk(0, 0, 0);
+    float pdf_brdf = ndotl / 3.14159265f;
+    float pdf_light;
+    if (l->kind == PGPU_LIGHT_POINT && l->radius > 0.0f) {
+        float r = l->radius;
+        float cos_at_light = dot(mk(-L.x, -L.y, -L.z), mk(0, 1, 0));
+        if (cos_at_light < 0.01f) cos_at_light = 0.01f;
+        pdf_light = (dist * dist) / (3.14159265f * r * r * cos_at_light);
+    } else {
+        pdf_light = 1.0f;
+    }
+    float w_light = (pdf_light * pdf_light) / (pdf_light * pdf_light + pdf_brdf * pdf_brdf + 1e-9f);
+    float w_brdf = 1.0f - w_light;
+    v3 nee = mulf(mulv(albedo, ld3(l->intensity)), ndotl);
+    v3 brdf = mulv(albedo, ld3(l->intensity));
+    return mulv(T, add(mulf(nee, w_light), mulf(brdf, w_brdf)));
+}
+
 static v3 trace_path(ctx_t* c, ray_t r, int bounces, rng_t* rng) {
     const orc_scene* s = c->s;
     float bias = c->p->shadow_bias;
@@ -550,7 +576,8 @@ static v3 trace_path(ctx_t* c, ray_t r, int bounces, rng_t* rng) {
             ray_t sr = {add(rec.p, mulf(rec.n, bias)), L};
             if (!l->is_emissive && scene_occ(&c->tv, sr, bias, dist - bias)) continue;
             float ndotl = clampf(dot(sn, L), 0.0f, 1.0f);
-            rad = add(rad, mulf(mulv(mulv(T, albedo), ld3(l->intensity)), ndotl));
+            rad = add(rad, light_term(l, (c->p->flags & PGPU_FLAG_MIS) != 0, T, albedo, L, dist,
+                                      ndotl));
         }
         rad = add(rad, mulv(mulv(T, albedo), ld3(s->ambient)));
         if (bounces - depth > 3) {
@@ -773,7 +800,7 @@ static int split_vertex(split_t* sp, ray_t* ray, v3* T, v3* L, rng_t* rng, int* 
             v3 Ld; float dist;
             light_dir(l, h->p, rng, &Ld, &dist);
             float ndotl = clampf(dot(h->n, Ld), 0.0f, 1.0f);
-            v3 cc = mulf(mulv(mulv(*T, albedo), ld3(l->intensity)), ndotl);
+            v3 cc = light_term(l, (P->flags & PGPU_FLAG_MIS) != 0, *T, albedo, Ld, dist, ndotl);
             ray_t sr = {sorg, Ld};
             int vis = l->is_emissive || !scene_occ(&c->tv, sr, P->shadow_bias, dist - P->shadow_bias);
             nee_add(&acc, L, cc, 0, vis);

@@ -208,13 +208,15 @@ def ref_dump(scene) -> tuple[np.ndarray, np.ndarray, int]:
 
 def ref_render(scene, width: int, height: int, samples: int, depth: int, pathtrace: bool,
                threads: int = 8, repeat: int = 1, bias: float = 1e-3, soft: int = 4,
-               want_image: bool = True):
-    """Render with the reference's Renderer::render; returns (image, info)."""
+               want_image: bool = True, mis: bool = False):
+    """Render with the reference's Renderer::render; returns (image, info).
+    mis: path tracing with RenderSettings::mis (trace_path_mis)."""
     with tempfile.TemporaryDirectory() as d:
         sp, op = Path(d) / "s.bin", Path(d) / "img.f32"
         scene.write(sp)
         out = _run_ref(["render", str(sp), str(op) if want_image else "-", str(width),
-                        str(height), str(samples), str(depth), "0" if pathtrace else "1",
+                        str(height), str(samples), str(depth),
+                        ("2" if mis else "0") if pathtrace else "1",
                         repr(float(bias)), str(soft), str(threads), str(repeat)])
         info = json.loads(out.strip().splitlines()[-1])
         img = (np.fromfile(op, np.float32).reshape(height, width, 3) if want_image else None)

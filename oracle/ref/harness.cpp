@@ -5,7 +5,8 @@
 // Commands (all binary files little-endian, formats in scene_io below):
 //   dump   <scene.bin> <out.bin>        stored primitive state + DFS BVH
 //   render <scene.bin> <out.f32> W H n depth mode bias soft threads repeat
-//                                       mode 0 = trace_path, 1 = Whitted;
+//                                       mode 0 = trace_path, 1 = Whitted,
+//                                       2 = trace_path_mis;
 //                                       prints {"seconds":[...],"rays":N}
 //   hits   <scene.bin> <rays.f32> <out.bin>   closest hit per ray
 //   parse  <file.pecl> <out_scene.bin>  reference parser -> scene file,
@@ -284,7 +285,10 @@ int cmd_render(int argc, char** argv) {
     rs.height = std::atoi(argv[5]);
     rs.samples = std::atoi(argv[6]);
     rs.max_depth = std::atoi(argv[7]);
-    rs.pathtrace = std::atoi(argv[8]) == 0;
+    // mode: 0 path tracing (trace_path), 1 Whitted (trace), 2 path tracing
+    // with multiple importance sampling (trace_path_mis)
+    rs.pathtrace = std::atoi(argv[8]) != 1;
+    rs.mis = std::atoi(argv[8]) == 2;
     rs.pathtrace_bounces = rs.max_depth;
     rs.shadow_bias = (float)std::atof(argv[9]);
     rs.soft_shadow_samples = std::atoi(argv[10]);

@@ -36,6 +36,7 @@ GLASS_FRESNEL_SPLIT, GLASS_BOTH_BRANCHES = 0, 1
 FLAG_DEVICE_OUTPUT, FLAG_COUNT_RAYS, FLAG_COUNT_NODES, FLAG_NO_GRAPH = 1, 2, 4, 8
 FLAG_PROFILE_KERNELS = 16
 FLAG_NO_PACKETS = 32
+FLAG_MIS = 64
 KERNEL_CLASSES = ("generate", "extend", "shade", "shadow", "accumulate", "megakernel")
 
 PRIM_DTYPE = np.dtype([("type", "<i4"), ("material", "<i4"), ("p", "<f4", (14,))])

@@ -162,9 +162,9 @@ inline bool describe(const pencil::ParsedScene& ps, SceneTables& t, std::string&
 // wavefront engine with the counter RNG (same expectation, faster).
 inline bool params_of(const pencil::RenderSettings& rs, pgpu_render_params& p, std::string& why) {
     if (rs.normals_mode || rs.bloom || rs.denoise || rs.bdpt || rs.spectral || rs.volume ||
-        rs.sss_enabled || rs.mis || rs.god_rays || rs.motion_blur || rs.adaptive ||
-        rs.caustics || rs.ppm) {
-        why = "only the plain path tracer and the Whitted tracer run on the GPU";
+        rs.sss_enabled || rs.god_rays || rs.motion_blur || rs.adaptive || rs.caustics ||
+        rs.ppm) {
+        why = "only the path tracer (plain or MIS) and the Whitted tracer run on the GPU";
         return false;
     }
     p = pgpu_render_params{};
@@ -175,6 +175,7 @@ inline bool params_of(const pencil::RenderSettings& rs, pgpu_render_params& p, s
     p.depth = rs.pathtrace ? rs.pathtrace_bounces : rs.max_depth;
     p.shadow_bias = rs.shadow_bias;
     p.soft_shadow_samples = rs.soft_shadow_samples;
+    if (rs.pathtrace && rs.mis) p.flags |= PGPU_FLAG_MIS;   // trace_path_mis (renderer.hpp:341)
     const char* exact = std::getenv("PENCIL_GPU_EXACT");
     if (exact && exact[0] == '1') {
         p.engine = PGPU_ENGINE_MEGAKERNEL;

@@ -371,7 +371,7 @@ cudaError_t launch_adjoint(const SceneView& S, const RenderCfg& c, const float* 
     AdjArgs A;
     A.S = S;
     A.P = PathParams{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias,
-                     c.salt, c.sample_offset};
+                     c.salt, c.sample_offset, 0};
     int G = 1;
     int lim = c.spp < 32 ? c.spp : 32;
     while (G * 2 <= lim) G *= 2;

@@ -791,6 +791,7 @@ int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, Re
     cfg.sort_key = p->sort_key;
     cfg.profile = (p->flags & PGPU_FLAG_PROFILE_KERNELS) != 0;
     cfg.packets = (p->flags & PGPU_FLAG_NO_PACKETS) == 0;
+    cfg.mis = (p->flags & PGPU_FLAG_MIS) != 0;
     (void)ds;
     return PGPU_OK;
 }
@@ -995,6 +996,8 @@ int32_t pgpu_adjoint(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, const
         return fail(c, PGPU_ERR_UNSUPPORTED, "the adjoint replays the counter-RNG, Fresnel-split estimator");
     if (cfg.depth > adjoint_max_depth())
         return fail(c, PGPU_ERR_UNSUPPORTED, "adjoint depth is limited to %d", adjoint_max_depth());
+    if (cfg.mis)
+        return fail(c, PGPU_ERR_UNSUPPORTED, "the adjoint replays trace_path's light weights, not MIS");
     if ((int)ds->lights.size() > adjoint_max_lights())
         return fail(c, PGPU_ERR_UNSUPPORTED, "adjoint supports at most %d lights", adjoint_max_lights());
     PGPU_CUDA(c, cudaSetDevice(c->device));

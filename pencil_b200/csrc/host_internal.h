@@ -38,6 +38,7 @@ struct RenderCfg {
     int sort_key;
     bool profile;
     bool packets;     // wavefront: camera rays of a one-scene frame as warp packets
+    bool mis;         // trace_path_mis's light weights
 };
 
 // Device counters written by the kernels (atomic adds).

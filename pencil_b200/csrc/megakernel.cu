@@ -103,7 +103,7 @@ static cudaError_t launch_mk(const SceneView& S, const PathParams& P, int G, flo
 cudaError_t launch_megakernel(const SceneView& S, const RenderCfg& c, float* out, float* m2,
                               unsigned long long* counters, cudaStream_t st) {
     PathParams P{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias, c.salt,
-                 c.sample_offset};
+                 c.sample_offset, c.mis ? 1 : 0};
     const bool seq = c.rng == PGPU_RNG_PIXEL_SEQUENTIAL;
     const bool tree = c.glass == PGPU_GLASS_BOTH_BRANCHES;
     int G = 1;

@@ -15,6 +15,7 @@ struct PathParams {
     float bias;
     uint32_t salt;
     int sample_offset;
+    int mis;          // 1: trace_path_mis's light weights (src/renderer.hpp:1205-1346)
 };
 
 enum { kModePT = 0, kModeWhitted = 1 };
@@ -49,6 +50,34 @@ __device__ __forceinline__ void light_dir(const DevLight& l, V3 p, Rng& rng, V3&
         L = -ld3(l.pos);
         dist = 1e9f;
     }
+}
+
+// Contribution of a visible point/directional light sample at a path-trace
+// vertex. trace_path (src/renderer.hpp:912-913): T * albedo * I * (n.L).
+// trace_path_mis (src/renderer.hpp:1264-1297): the power-heuristic mix of the
+// light-sampled term albedo * I * (n.L) and the BSDF-sampled term albedo * I,
+// with a disc light's pdf taken for a light facing down (axis +y, cosine at
+// least 0.01), and nothing when n.L <= 0.
+__device__ __forceinline__ V3 light_term(const DevLight& l, bool mis, V3 T, V3 albedo, V3 L,
+                                         float dist, float ndotl) {
+    if (!mis) return T * albedo * ld3(l.intensity) * ndotl;
+    if (ndotl <= 0.0f) return v3(0.0f, 0.0f, 0.0f);
+    const float pdf_brdf = ndotl / 3.14159265f;
+    float pdf_light;
+    if (l.kind == 0 && l.radius > 0.0f) {
+        const float r = l.radius;
+        float cos_at_light = dot(-L, v3(0.0f, 1.0f, 0.0f));
+        if (cos_at_light < 0.01f) cos_at_light = 0.01f;
+        pdf_light = (dist * dist) / (3.14159265f * r * r * cos_at_light);
+    } else {
+        pdf_light = 1.0f;
+    }
+    const float w_light =
+        (pdf_light * pdf_light) / (pdf_light * pdf_light + pdf_brdf * pdf_brdf + 1e-9f);
+    const float w_brdf = 1.0f - w_light;
+    const V3 nee = albedo * ld3(l.intensity) * ndotl;
+    const V3 brdf = albedo * ld3(l.intensity);
+    return T * (nee * w_light + brdf * w_brdf);
 }
 
 // trace_dielectric's two rays and Fresnel weight (src/renderer.hpp:1582-1627).
@@ -212,7 +241,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& S, const PathParam
             light_dir(l, h.p, ps.rng, L, dist);
             float ndotl = clampf(dot(h.n, L), 0.0f, 1.0f);
             E.shadow(ps.L, Ray{sorg, L}, P.bias, dist - P.bias, !l.is_emissive,
-                     ps.T * albedo * ld3(l.intensity) * ndotl, 0);
+                     light_term(l, P.mis != 0, ps.T, albedo, L, dist, ndotl), 0);
         }
         if (S.has_quad_lights && diffuse && ps.depth - 1 > 0) {
             for (int li = 0; li < S.n_lights; ++li) {
@@ -501,7 +530,7 @@ struct Tracer {
             Ray sr{h.p + h.n * P.bias, L};
             if (!l.is_emissive && occluded(sr, P.bias, dist - P.bias)) continue;
             float ndotl = clampf(dot(h.n, L), 0.0f, 1.0f);
-            rad = rad + T * albedo * ld3(l.intensity) * ndotl;
+            rad = rad + light_term(l, P.mis != 0, T, albedo, L, dist, ndotl);
         }
         if (quad_nee) {
             for (int li = 0; li < S.n_lights; ++li) {

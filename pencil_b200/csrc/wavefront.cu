@@ -1018,7 +1018,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
         const RenderCfg& c = cfgs[k];
         WfJob& J = jobs[k];
         J.P = PathParams{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias,
-                         c.salt, c.sample_offset};
+                         c.salt, c.sample_offset, c.mis ? 1 : 0};
         J.view = job_view[k];
         J.path_off = path_off;
         J.pix_off = pix_off;
@@ -1239,7 +1239,7 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
     A.refill_below = kDefaultRefill;
     WfJob J;
     J.P = PathParams{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias,
-                     c.salt, c.sample_offset};
+                     c.salt, c.sample_offset, c.mis ? 1 : 0};
     J.view = 0;
     J.path_off = 0;
     J.pix_off = 0;

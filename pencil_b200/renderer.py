@@ -44,6 +44,7 @@ class RenderSettings:
     use_graph: bool = True
     profile_kernels: bool = False
     packets: bool = True           # wavefront: camera rays traced as warp packets
+    mis: bool = False              # trace_path_mis's light weights (Pencil's `mis`)
     queue_capacity: int = 0
     sort_key: int = 0
     refill_below: int = 0
@@ -62,7 +63,8 @@ class RenderSettings:
                    (A.FLAG_COUNT_NODES if self.count_nodes else 0) |
                    (0 if self.use_graph else A.FLAG_NO_GRAPH) |
                    (A.FLAG_PROFILE_KERNELS if self.profile_kernels else 0) |
-                   (0 if self.packets else A.FLAG_NO_PACKETS))
+                   (0 if self.packets else A.FLAG_NO_PACKETS) |
+                   (A.FLAG_MIS if self.mis else 0))
         p.queue_capacity, p.sort_key = self.queue_capacity, self.sort_key
         p.refill_below = self.refill_below
         return p

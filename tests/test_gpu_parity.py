@@ -14,6 +14,8 @@ Bars:
 """
 from __future__ import annotations
 
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -212,6 +214,29 @@ def test_production_estimator_matches_oracle_path_for_path(gpu, scenes, name, mo
     st.samples = 4
     ref, _, _ = O.Oracle(scene, fx["nodes"], fx["prims"]).render_split(st)
     near_exact(gpu.render(sid, st), ref)
+
+
+@pytest.mark.parametrize("seed", [15, 16, 17])
+def test_mis_path_tracing(gpu, seed):
+    """RenderSettings::mis (trace_path_mis, src/renderer.hpp:1205-1346) on
+    seeded scenes with disc, point and directional lights: the megakernel
+    with Pencil's RNG equals the oracle (which equals the reference bit for
+    bit, test_oracle_live_ref.py); the wavefront equals the megakernel; the
+    production estimator equals the oracle's restatement of it."""
+    from test_oracle_live_ref import random_scene
+    s = random_scene(seed, 60)
+    sid = gpu.upload(s)
+    st = RenderSettings(width=40, height=30, samples=2, max_depth=6, pathtrace=True,
+                        pathtrace_bounces=6, mis=True)
+    ref, _, _ = O.Oracle(s).render(st)
+    near_exact(gpu.render(sid, exact_mode(dataclasses.replace(st))), ref)
+    mk = gpu.render(sid, dataclasses.replace(st, engine=A.ENGINE_MEGAKERNEL))
+    wf = gpu.render(sid, dataclasses.replace(st, engine=A.ENGINE_WAVEFRONT))
+    assert np.array_equal(mk.view(np.uint32), wf.view(np.uint32))
+    split, _, _ = O.Oracle(s).render_split(st)
+    near_exact(wf, split)
+    assert not np.array_equal(wf, gpu.render(sid, dataclasses.replace(st, mis=False)))
+    gpu.free(sid)
 
 
 @pytest.mark.parametrize("name", ["c1", "cloud2k", "prims_mix", "cornell_box"])

@@ -3,6 +3,8 @@
 `make -C oracle`). Skipped where that binary is absent."""
 from __future__ import annotations
 
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -102,6 +104,21 @@ def test_oracle_render_matches_reference(seed, pathtrace):
     ref, info = O.ref_render(s, 40, 30, 2, 6, pathtrace)
     assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
     assert int(cnt[O.CNT_REFERENCE_RAYS]) == info["rays"]
+
+
+@pytest.mark.parametrize("seed", [15, 16, 17])
+def test_oracle_mis_render_matches_reference(seed):
+    """Path tracing with RenderSettings::mis (trace_path_mis): disc, point and
+    directional lights, bit for bit, same ray count."""
+    s = random_scene(seed, 60)
+    st = RenderSettings(width=40, height=30, samples=2, max_depth=6, pathtrace=True,
+                        pathtrace_bounces=6, mis=True)
+    img, _, cnt = O.Oracle(s).render(st)
+    ref, info = O.ref_render(s, 40, 30, 2, 6, True, mis=True)
+    assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+    assert int(cnt[O.CNT_REFERENCE_RAYS]) == info["rays"]
+    plain, _, _ = O.Oracle(s).render(dataclasses.replace(st, mis=False))
+    assert not np.array_equal(img, plain)        # the weights changed the image
 
 
 @pytest.mark.parametrize("seed", [21, 22])
