@@ -385,6 +385,19 @@ int32_t pgpu_render_noalloc(pgpu_ctx* ctx, int32_t scene_id,
                             const pgpu_render_params* params,
                             float* out_rgb_device, float* out_m2_device);
 
+/* Pencil's output path on the device: exposure, tone curve, clamp, gamma 2.2
+ * and 8 bits per channel, the bytes write_image / color_to_rgb8 produce
+ * (src/image_io.hpp:40-113, src/tonemap.hpp:27-61) for the same HDR input.
+ * tonemap: 0 none, 1 ACES (Pencil's default), 2 Reinhard; exposure in stops.
+ * hdr: n_pixels*3 floats, out_rgb8: n_pixels*3 bytes; with
+ * PGPU_TONEMAP_DEVICE_INPUT / _OUTPUT the pointers are device memory. */
+enum pgpu_tonemap_flags {
+    PGPU_TONEMAP_DEVICE_INPUT  = 1,
+    PGPU_TONEMAP_DEVICE_OUTPUT = 2
+};
+int32_t pgpu_tonemap(pgpu_ctx* ctx, const float* hdr, int32_t n_pixels, int32_t tonemap,
+                     float exposure, int32_t flags, uint8_t* out_rgb8);
+
 /* Replace material table entries of an uploaded scene (same count), e.g.
  * between inverse-rendering steps. */
 int32_t pgpu_update_materials(pgpu_ctx* ctx, int32_t scene_id,

@@ -1557,3 +1557,20 @@ void orc_rgb8(const float* hdr, int32_t n_pixels, uint8_t* out, int32_t tonemap,
         }
     }
 }
+
+/* Checks that the 8-bit gamma step of write_image (src/image_io.hpp:88-97),
+ * x -> (uint8)(pow(clamp(x, 0, 1), 1/2.2) * 255 + 0.5) with this host's powf,
+ * never decreases over all floats in [0, 1] (in bit order). Returns 0, or the
+ * bit pattern after which it first decreased. */
+uint32_t orc_gamma_monotone(void) {
+    uint8_t prev = 0;
+    for (uint32_t b = 0; b <= 0x3f800000u; ++b) {
+        float x;
+        memcpy(&x, &b, 4);
+        float g = powf(clampf(x, 0.0f, 1.0f), 1.0f / 2.2f);
+        uint8_t q = (uint8_t)(g * 255.0f + 0.5f);
+        if (q < prev) return b;
+        prev = q;
+    }
+    return 0;
+}

@@ -101,6 +101,7 @@ double orc_hit_t_fp64(const pgpu_prim* prim, const float* ray);
 
 /* HDR -> 8-bit RGB as write_image does. tonemap: 0 none, 1 ACES,
  * 2 Reinhard. */
+uint32_t orc_gamma_monotone(void);
 void orc_rgb8(const float* hdr, int32_t n_pixels, uint8_t* out,
               int32_t tonemap, float exposure);
 

@@ -68,6 +68,8 @@ def load():
     lib.orc_hit_t_fp64.argtypes = [C.c_void_p, C.c_void_p]
     lib.orc_hit_t_fp64.restype = C.c_double
     lib.orc_rgb8.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_float]
+    lib.orc_gamma_monotone.restype = C.c_uint32
+    lib.orc_gamma_monotone.argtypes = []
     lib.orc_path_seed.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_uint32]
     lib.orc_path_seed.restype = C.c_uint32
     _lib = lib
@@ -166,6 +168,12 @@ class Oracle:
         ray = np.ascontiguousarray(ray, np.float32).reshape(6)
         rec = np.ascontiguousarray(self.prims[prim_id:prim_id + 1])
         return self.lib.orc_hit_t_fp64(A.ptr(rec), A.ptr(ray))
+
+
+def gamma_monotone() -> int:
+    """0 when write_image's gamma byte never decreases over the floats of
+    [0, 1] with this host's powf (else the bit pattern where it first does)."""
+    return int(load().orc_gamma_monotone())
 
 
 def rgb8(hdr: np.ndarray, tonemap: int = 1, exposure: float = 0.0) -> np.ndarray:

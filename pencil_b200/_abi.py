@@ -37,6 +37,8 @@ FLAG_DEVICE_OUTPUT, FLAG_COUNT_RAYS, FLAG_COUNT_NODES, FLAG_NO_GRAPH = 1, 2, 4, 
 FLAG_PROFILE_KERNELS = 16
 FLAG_NO_PACKETS = 32
 FLAG_MIS = 64
+TONEMAP_NONE, TONEMAP_ACES, TONEMAP_REINHARD = 0, 1, 2
+TONEMAP_DEVICE_INPUT, TONEMAP_DEVICE_OUTPUT = 1, 2
 KERNEL_CLASSES = ("generate", "extend", "shade", "shadow", "accumulate", "megakernel")
 
 PRIM_DTYPE = np.dtype([("type", "<i4"), ("material", "<i4"), ("p", "<f4", (14,))])
@@ -129,6 +131,8 @@ EXPORTS = {
                                  C.POINTER(Stats)]),
     "pgpu_update_materials": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
     "pgpu_get_scene_info": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(SceneInfo)]),
+    "pgpu_tonemap": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_float,
+                                 C.c_int32, C.c_void_p]),
     "pgpu_render_noalloc": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(RenderParams),
                                         C.c_void_p, C.c_void_p]),
 }

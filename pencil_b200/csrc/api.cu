@@ -45,6 +45,8 @@ cudaError_t launch_adjoint(const SceneView& S, const RenderCfg& c, const float* 
                            unsigned long long* counters, cudaStream_t st);
 int adjoint_max_depth();
 int adjoint_max_lights();
+cudaError_t launch_tonemap(const float* d_hdr, long long n_pixels, int mode, float exposure,
+                           uint8_t* d_out, cudaStream_t st);
 
 constexpr int kMaxDepth = 64;          // traversal stack bound (kMaxStack)
 constexpr int kMaxTreeFrames = 32;     // Whitted recursion bound of the two-branch mode
@@ -131,6 +133,8 @@ struct pgpu_ctx {
     size_t stage_cap = 0;
     unsigned char* d_adj = nullptr;   // adjoint inputs and gradient sums
     size_t adj_cap = 0;
+    uint8_t* d_rgb8 = nullptr;        // tonemap output staging
+    size_t rgb8_cap = 0;
     // scene arenas come from a stream-ordered pool owned by the context, so
     // that upload / free cycles reuse device memory without cudaMalloc or
     // cudaFree (each of which synchronises the device)
@@ -340,6 +344,7 @@ void pgpu_destroy(pgpu_ctx* c) {
     cudaFree(c->d_cnt);
     cudaFree(c->d_query);
     cudaFree(c->d_adj);
+    cudaFree(c->d_rgb8);
     wavefront_delete(c->wf);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -709,6 +714,37 @@ int32_t pgpu_get_scene_info(pgpu_ctx* c, int32_t id, pgpu_scene_info* out) {
     info.bvh_depth = ds->depth;
     info.wide_stack = ds->wide_stack;
     *out = info;
+    return PGPU_OK;
+}
+
+int32_t pgpu_tonemap(pgpu_ctx* c, const float* hdr, int32_t n_pixels, int32_t tonemap,
+                     float exposure, int32_t flags, uint8_t* out_rgb8) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    if (!hdr || !out_rgb8 || n_pixels < 0)
+        return fail(c, PGPU_ERR_INVALID_ARG, "null buffer or negative pixel count");
+    if (tonemap < 0 || tonemap > 2)
+        return fail(c, PGPU_ERR_UNSUPPORTED, "tone map %d (0 none, 1 ACES, 2 Reinhard)", tonemap);
+    if (!std::isfinite(exposure)) return fail(c, PGPU_ERR_INVALID_ARG, "exposure is not finite");
+    if (n_pixels == 0) return PGPU_OK;
+    PGPU_CUDA(c, cudaSetDevice(c->device));
+    const size_t n3 = (size_t)n_pixels * 3;
+    const float* d_in = hdr;
+    if (!(flags & PGPU_TONEMAP_DEVICE_INPUT)) {
+        int rc = ensure(c, c->d_out, c->out_cap, n3 * 4);
+        if (rc) return rc;
+        PGPU_CUDA(c, cudaMemcpyAsync(c->d_out, hdr, n3 * 4, cudaMemcpyHostToDevice, c->stream));
+        d_in = c->d_out;
+    }
+    uint8_t* d_dst = out_rgb8;
+    if (!(flags & PGPU_TONEMAP_DEVICE_OUTPUT)) {
+        int rc = ensure(c, c->d_rgb8, c->rgb8_cap, n3);
+        if (rc) return rc;
+        d_dst = c->d_rgb8;
+    }
+    PGPU_CUDA(c, launch_tonemap(d_in, n_pixels, tonemap, exposure, d_dst, c->stream));
+    if (!(flags & PGPU_TONEMAP_DEVICE_OUTPUT))
+        PGPU_CUDA(c, cudaMemcpyAsync(out_rgb8, d_dst, n3, cudaMemcpyDeviceToHost, c->stream));
+    PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     return PGPU_OK;
 }
 

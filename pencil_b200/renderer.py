@@ -154,6 +154,16 @@ class GpuContext:
         return {name: int(getattr(info, name)) for name, _ in A.SceneInfo._fields_
                 if name != "reserved"}
 
+    def tonemap(self, hdr: np.ndarray, tonemap: int = A.TONEMAP_ACES,
+                exposure: float = 0.0) -> np.ndarray:
+        """Pencil's write_image bytes (exposure, tone curve, gamma 2.2, 8 bits)
+        computed on the device from a host HDR image (H, W, 3)."""
+        hdr = np.ascontiguousarray(hdr, np.float32)
+        out = np.empty(hdr.shape, np.uint8)
+        self.check(self.lib.pgpu_tonemap(self.h, A.ptr(hdr), hdr.size // 3, tonemap,
+                                         float(exposure), 0, A.ptr(out)), "pgpu_tonemap")
+        return out
+
     def update_materials(self, sid: int, mats: np.ndarray) -> None:
         mats = np.ascontiguousarray(mats, A.MATERIAL_DTYPE)
         self.check(self.lib.pgpu_update_materials(self.h, sid, A.ptr(mats), len(mats)),
