@@ -474,6 +474,41 @@ def measure_extras(ctx, sid, st, img, stream) -> dict:
     for s_ in sids:
         ctx.free(s_)
     out["mesh"] = measure_mesh(ctx, stream)
+    out["bvh_build"] = measure_bvh_build(ctx, stream)
+    return out
+
+
+def measure_bvh_build(ctx, stream) -> dict:
+    """Pencil's host SAH build against the device LBVH build, and the render
+    time on each tree (sphere cloud, tuned launch parameters)."""
+    import time
+
+    import torch
+    from pencil_b200 import _abi as A
+    from pencil_b200 import workloads as W
+    out = {}
+    for name, wl in (("sphere_cloud", W.sphere_cloud()), ("mesh_box", W.mesh_box())):
+        t0 = time.perf_counter()
+        host_nodes, host_depth = wl.scene.build_bvh()
+        host_ms = (time.perf_counter() - t0) * 1e3
+        ctx.build_bvh_device(wl.scene)                      # first call loads the module
+        t0 = time.perf_counter()
+        dev_nodes, dev_depth = ctx.build_bvh_device(wl.scene)
+        dev_ms = (time.perf_counter() - t0) * 1e3
+        rec = {"primitives": wl.scene.n_unified, "host_sah_ms": host_ms, "host_depth": host_depth,
+               "device_lbvh_ms": dev_ms, "device_depth": dev_depth}
+        if name == "sphere_cloud":
+            st = wl.settings
+            st.engine = A.ENGINE_WAVEFRONT
+            st.queue_capacity = st.width * st.height * st.samples ** 2
+            st.refill_below, st.sort_key = 16, 2
+            buf = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")
+            for tree, nodes in (("sah", host_nodes), ("lbvh", dev_nodes)):
+                sid = ctx.upload(wl.scene, nodes)
+                rec[f"render_ms_{tree}"] = _event_ms(
+                    stream, lambda: ctx.render_device(sid, st, buf.data_ptr()), 3)
+                ctx.free(sid)
+        out[name] = rec
     return out
 
 

@@ -296,6 +296,18 @@ int32_t pgpu_make_prim(int32_t type, int32_t material, const float* a,
 int32_t pgpu_build_bvh(const pgpu_scene* scene, pgpu_bvh_node* out_nodes,
                        int32_t* out_n_nodes, int32_t* out_depth);
 
+/* A BVH built on the GPU in the same table format (DFS pre-order, one
+ * primitive per leaf): a linear BVH over the Morton codes of the primitive
+ * boxes' centres (Karras 2012), for scenes whose host SAH build
+ * (pgpu_build_bvh, Pencil's tree) costs too much, e.g. many scenes or every
+ * frame of an animation. No counterpart in the reference, which builds on
+ * the host only (src/bvh.hpp:54-192). It is a different tree: renders agree
+ * with those on Pencil's tree up to hit ties within rounding. out_nodes NULL:
+ * *out_n_nodes gets the table size only. */
+int32_t pgpu_build_bvh_device(pgpu_ctx* ctx, const pgpu_scene* scene,
+                              pgpu_bvh_node* out_nodes, int32_t* out_n_nodes,
+                              int32_t* out_depth);
+
 /* Upload a scene; returns a scene id valid until pgpu_free_scene. */
 int32_t pgpu_upload_scene(pgpu_ctx* ctx, const pgpu_scene* scene,
                           int32_t* out_scene_id);

@@ -21,7 +21,7 @@ LIB = HERE / "libpencil_gpu.so"
 INCLUDE = HERE.parent / "include"
 
 CU_SOURCES = ["api.cu", "megakernel.cu", "wavefront.cu", "queries.cu", "adjoint.cu",
-              "tonemap.cu"]
+              "tonemap.cu", "bvh_device.cu"]
 CXX_SOURCES = ["bvh_build.cpp", "bvh_wide.cpp"]
 HEADERS = ["device_common.cuh", "path.cuh", "scene_layout.h", "host_internal.h"]
 

@@ -47,6 +47,8 @@ int adjoint_max_depth();
 int adjoint_max_lights();
 cudaError_t launch_tonemap(const float* d_hdr, long long n_pixels, int mode, float exposure,
                            uint8_t* d_out, cudaStream_t st);
+cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_node>& out,
+                        int& depth, cudaStream_t st);
 
 constexpr int kMaxDepth = 64;          // traversal stack bound (kMaxStack)
 constexpr int kMaxTreeFrames = 32;     // Whitted recursion bound of the two-branch mode
@@ -386,6 +388,44 @@ int32_t pgpu_build_bvh(const pgpu_scene* s, pgpu_bvh_node* out_nodes, int32_t* o
     build_bvh(prims, nodes, depth);
     if (out_nodes) std::memcpy(out_nodes, nodes.data(), nodes.size() * sizeof(pgpu_bvh_node));
     *out_n_nodes = (int32_t)nodes.size();
+    if (out_depth) *out_depth = depth;
+    return PGPU_OK;
+}
+
+int32_t pgpu_build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node* out_nodes,
+                              int32_t* out_n_nodes, int32_t* out_depth) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    if (!s || !out_n_nodes || (s->n_prims > 0 && !s->prims) || s->n_prims < 0 ||
+        s->n_mesh_triangles < 0 || s->n_mesh_vertices < 0 ||
+        (s->n_mesh_triangles > 0 && (!s->mesh_indices || !s->mesh_vertices)))
+        return fail(c, PGPU_ERR_INVALID_ARG, "bad scene arrays");
+    const long long n_unified = (long long)s->n_prims + s->n_mesh_triangles;
+    if (n_unified >= kMaxLeaves) return fail(c, PGPU_ERR_UNSUPPORTED, "too many primitives");
+    {
+        const int bad = first_bad(3 * s->n_mesh_triangles, [&](int k) {
+            return s->mesh_indices[k] < 0 || s->mesh_indices[k] >= s->n_mesh_vertices;
+        });
+        if (bad >= 0) return fail(c, PGPU_ERR_INVALID_ARG, "mesh index %d out of range", bad);
+    }
+    const int n = (int)n_unified;
+    *out_n_nodes = n ? 2 * n - 1 : 0;
+    if (!out_nodes) return PGPU_OK;           // size query
+    if (n <= 1) {                             // nothing to build: the host does it
+        std::vector<pgpu_prim> prims;
+        unified_prims(*s, prims);
+        std::vector<pgpu_bvh_node> nodes;
+        int depth = 0;
+        build_bvh(prims, nodes, depth);
+        std::memcpy(out_nodes, nodes.data(), nodes.size() * sizeof(pgpu_bvh_node));
+        if (out_depth) *out_depth = depth;
+        return PGPU_OK;
+    }
+    PGPU_CUDA(c, cudaSetDevice(c->device));
+    std::vector<pgpu_bvh_node> nodes;
+    int depth = 0;
+    cudaError_t e = device_lbvh(*s, n, nodes, depth, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "device BVH build");
+    std::memcpy(out_nodes, nodes.data(), nodes.size() * sizeof(pgpu_bvh_node));
     if (out_depth) *out_depth = depth;
     return PGPU_OK;
 }

@@ -145,6 +145,19 @@ class GpuContext:
     def free(self, sid: int) -> None:
         self.check(self.lib.pgpu_free_scene(self.h, sid), "pgpu_free_scene")
 
+    def build_bvh_device(self, scene: Scene) -> tuple[np.ndarray, int]:
+        """A linear BVH built on the GPU, in the node-table format of
+        Scene.build_bvh (DFS pre-order); returns (nodes, depth)."""
+        d, keep = scene.desc()
+        n = scene.n_unified
+        nodes = np.zeros(max(2 * n - 1, 1), A.NODE_DTYPE)
+        cnt, depth = C.c_int32(0), C.c_int32(0)
+        self.check(self.lib.pgpu_build_bvh_device(self.h, C.byref(d), A.ptr(nodes),
+                                                  C.byref(cnt), C.byref(depth)),
+                   "pgpu_build_bvh_device")
+        del keep
+        return nodes[: cnt.value].copy(), depth.value
+
     def scene_info(self, sid: int) -> dict:
         """Sizes of an uploaded scene (device bytes, leaves, binary and wide
         node counts, depth, wide-tree stack need)."""
