@@ -397,6 +397,16 @@ int32_t pgpu_render_noalloc(pgpu_ctx* ctx, int32_t scene_id,
                             const pgpu_render_params* params,
                             float* out_rgb_device, float* out_m2_device);
 
+/* One tile of the distributed worker (render_tile, src/distributed.hpp:
+ * 380-434): params.width/height are the full image, out_rgb receives
+ * tile_w*tile_h*3 floats of pixels [tile_x, tile_x+tile_w) x [tile_y,
+ * tile_y+tile_h), each seeded and jittered as render_tile does (half-pixel
+ * jitter). The worker traces with the Whitted tracer (params.mode
+ * PGPU_MODE_WHITTED, depth = max_depth). Runs on the megakernel. */
+int32_t pgpu_render_tile(pgpu_ctx* ctx, int32_t scene_id, const pgpu_render_params* params,
+                         int32_t tile_x, int32_t tile_y, int32_t tile_w, int32_t tile_h,
+                         float* out_rgb);
+
 /* Pencil's output path on the device: exposure, tone curve, clamp, gamma 2.2
  * and 8 bits per channel, the bytes write_image / color_to_rgb8 produce
  * (src/image_io.hpp:40-113, src/tonemap.hpp:27-61) for the same HDR input.

@@ -703,6 +703,45 @@ int32_t orc_render(const orc_scene* s, const pgpu_render_params* p, float* out_r
     return 0;
 }
 
+/* The distributed worker's tile (render_tile, src/distributed.hpp:380-434):
+ * pixels of the full W x H image seeded as render_tile_region does, jittered
+ * by half a pixel, traced with trace (Whitted) to p->depth. */
+int32_t orc_render_tile(const orc_scene* s, const pgpu_render_params* p, int32_t tx, int32_t ty,
+                        int32_t tw, int32_t th, float* out_rgb) {
+    if (!s || !p || !out_rgb || p->width <= 0 || p->height <= 0 || p->samples <= 0) return -1;
+    if (tw <= 0 || th <= 0 || tx < 0 || ty < 0 || tx + tw > p->width || ty + th > p->height)
+        return -1;
+    uint64_t cnt[ORC_CNT_N] = {0};
+    ctx_t c;
+    c.s = s;
+    c.p = p;
+    c.cnt = cnt;
+    c.tv.s = s;
+    c.tv.cnt = cnt;
+    const int W = p->width, H = p->height, n = p->samples;
+    for (int j = 0; j < th; ++j) {
+        for (int i = 0; i < tw; ++i) {
+            const int px = tx + i, py = ty + j;
+            rng_t rng = {(uint32_t)(px * 97861u + py * 1973u + 1u)};
+            v3 acc = mk(0, 0, 0);
+            for (int sy = 0; sy < n; ++sy) {
+                for (int sx = 0; sx < n; ++sx) {
+                    float u = (px + (sx + 0.5f) / n) / (float)W;
+                    float v = 1.0f - (py + (sy + 0.5f) / n) / (float)H;
+                    u += rng_sym(&rng) * (0.5f / W);
+                    v += rng_sym(&rng) * (0.5f / H);
+                    ray_t r = camera_ray(s, u, v);
+                    acc = add(acc, whitted(&c, r, p->depth, &rng));
+                }
+            }
+            acc = divf(acc, (float)(n * n));
+            size_t o = ((size_t)j * tw + i) * 3;
+            out_rgb[o + 0] = acc.x; out_rgb[o + 1] = acc.y; out_rgb[o + 2] = acc.z;
+        }
+    }
+    return 0;
+}
+
 /* ---- the GPU core's single-ray estimator, restated ---------------------------
  * Test-only restatement of pencil_b200/csrc/path.cuh (shade_vertex, NeeAccum)
  * and of the megakernel's per-pixel accumulation: counter RNG seeded by

@@ -101,6 +101,8 @@ double orc_hit_t_fp64(const pgpu_prim* prim, const float* ray);
 
 /* HDR -> 8-bit RGB as write_image does. tonemap: 0 none, 1 ACES,
  * 2 Reinhard. */
+int32_t orc_render_tile(const orc_scene* s, const pgpu_render_params* p, int32_t tx, int32_t ty,
+                        int32_t tw, int32_t th, float* out_rgb);
 uint32_t orc_gamma_monotone(void);
 void orc_rgb8(const float* hdr, int32_t n_pixels, uint8_t* out,
               int32_t tonemap, float exposure);

@@ -70,6 +70,9 @@ def load():
     lib.orc_rgb8.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_float]
     lib.orc_gamma_monotone.restype = C.c_uint32
     lib.orc_gamma_monotone.argtypes = []
+    lib.orc_render_tile.restype = C.c_int32
+    lib.orc_render_tile.argtypes = [C.POINTER(OrcScene), C.POINTER(A.RenderParams), C.c_int32,
+                                    C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
     lib.orc_path_seed.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_uint32]
     lib.orc_path_seed.restype = C.c_uint32
     _lib = lib
@@ -125,6 +128,15 @@ class Oracle:
         if rc != 0:
             raise ValueError("orc_render_split rejected its arguments")
         return out, m2, cnt
+
+    def render_tile(self, settings, x: int, y: int, w: int, h: int) -> np.ndarray:
+        """The distributed worker's tile (render_tile) of the full image
+        that `settings` describe."""
+        p = settings.params()
+        out = np.zeros((h, w, 3), np.float32)
+        if self.lib.orc_render_tile(C.byref(self.s), C.byref(p), x, y, w, h, A.ptr(out)) != 0:
+            raise ValueError("orc_render_tile rejected its arguments")
+        return out
 
     def adjoint(self, settings, dl: np.ndarray, threads: int | None = None):
         """FP64 CPU adjoint of the production estimator: returns
@@ -240,6 +252,17 @@ def ref_hits(scene, rays: np.ndarray):
         raw = np.fromfile(op, np.int32)
     n = len(raw) // 2
     return raw[:n].copy(), raw[n:].view(np.float32).copy()
+
+
+def ref_tile(scene, width: int, height: int, x: int, y: int, w: int, h: int, samples: int,
+             depth: int, bias: float = 1e-3, soft: int = 4) -> np.ndarray:
+    """The reference worker's render_tile (src/distributed.hpp:380-434)."""
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = Path(d) / "s.bin", Path(d) / "tile.f32"
+        scene.write(sp)
+        _run_ref(["tile", str(sp), str(op), str(width), str(height), str(x), str(y), str(w),
+                  str(h), str(samples), str(depth), repr(float(bias)), str(soft)])
+        return np.fromfile(op, np.float32).reshape(h, w, 3)
 
 
 def ref_camrays(scene, uv: np.ndarray) -> np.ndarray:

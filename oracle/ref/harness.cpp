@@ -9,6 +9,8 @@
 //                                       2 = trace_path_mis;
 //                                       prints {"seconds":[...],"rays":N}
 //   hits   <scene.bin> <rays.f32> <out.bin>   closest hit per ray
+//   tile   <scene.bin> <out.f32> W H x y w h n depth bias soft
+//                                       the distributed worker's tile render
 //   parse  <file.pecl> <out_scene.bin>  reference parser -> scene file,
 //                                       prints the render block as JSON
 //
@@ -45,6 +47,7 @@
 #define protected public
 #include "pecl_parser.hpp"
 #include "renderer.hpp"
+#include "distributed.hpp"
 #undef private
 #undef protected
 
@@ -349,6 +352,31 @@ int cmd_hits(int argc, char** argv) {
     return 0;
 }
 
+// The distributed worker's tile render (render_tile, src/distributed.hpp:380-434).
+int cmd_tile(int argc, char** argv) {
+    if (argc < 14) return 2;
+    SceneFile sf;
+    if (!read_scene(argv[2], sf)) { std::fprintf(stderr, "cannot read scene\n"); return 2; }
+    Built b;
+    build_scene(sf, b, false);
+    const int W = std::atoi(argv[4]), H = std::atoi(argv[5]);
+    const int tx = std::atoi(argv[6]), ty = std::atoi(argv[7]);
+    const int tw = std::atoi(argv[8]), th = std::atoi(argv[9]);
+    RenderSettings rs;
+    rs.width = W;
+    rs.height = H;
+    rs.samples = std::atoi(argv[10]);
+    rs.max_depth = std::atoi(argv[11]);
+    rs.shadow_bias = (float)std::atof(argv[12]);
+    rs.soft_shadow_samples = std::atoi(argv[13]);
+    std::vector<Color> px;
+    render_tile(b.scene, b.camera, tx, ty, tw, th, W, H, rs.samples, rs.max_depth, px, &rs);
+    FILE* f = std::fopen(argv[3], "wb");
+    std::fwrite(px.data(), sizeof(Color), px.size(), f);
+    std::fclose(f);
+    return 0;
+}
+
 int cmd_camrays(int argc, char** argv) {
     // camrays <scene.bin> <uv.f32> <out.f32>: Camera::ray_at(u, v) per point
     if (argc < 5) return 2;
@@ -443,6 +471,7 @@ int main(int argc, char** argv) {
     if (c == "render") return cmd_render(argc, argv);
     if (c == "hits") return cmd_hits(argc, argv);
     if (c == "camrays") return cmd_camrays(argc, argv);
+    if (c == "tile") return cmd_tile(argc, argv);
     if (c == "parse") return cmd_parse(argc, argv);
     std::fprintf(stderr, "unknown command %s\n", argv[1]);
     return 2;

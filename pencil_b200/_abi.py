@@ -133,6 +133,8 @@ EXPORTS = {
     "pgpu_get_scene_info": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(SceneInfo)]),
     "pgpu_tonemap": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_float,
                                  C.c_int32, C.c_void_p]),
+    "pgpu_render_tile": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(RenderParams), C.c_int32,
+                                     C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     "pgpu_build_bvh_device": (C.c_int32, [C.c_void_p, C.POINTER(SceneDesc), C.c_void_p,
                                           C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "pgpu_render_noalloc": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(RenderParams),

@@ -21,7 +21,8 @@
 namespace pgpu {
 
 cudaError_t launch_megakernel(const SceneView& S, const RenderCfg& c, float* out, float* m2,
-                              unsigned long long* counters, cudaStream_t st);
+                              unsigned long long* counters, cudaStream_t st,
+                              const int* tile = nullptr);
 cudaError_t launch_query(const SceneView& S, bool camera, const float* in, int n, int* prim,
                          float* t, cudaStream_t st);
 
@@ -975,6 +976,39 @@ int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float*
         stats->total_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
+    return PGPU_OK;
+}
+
+int32_t pgpu_render_tile(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, int32_t tile_x,
+                         int32_t tile_y, int32_t tile_w, int32_t tile_h, float* out_rgb) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    DeviceScene* ds = find_scene(c, id);
+    if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
+    if (!out_rgb) return fail(c, PGPU_ERR_INVALID_ARG, "null output");
+    pgpu_render_params q = *p;
+    q.engine = PGPU_ENGINE_MEGAKERNEL;     // tiles run on the megakernel
+    RenderCfg cfg;
+    int rc = make_cfg(c, ds, &q, cfg);
+    if (rc) return rc;
+    if (tile_w <= 0 || tile_h <= 0 || tile_x < 0 || tile_y < 0 || tile_x + tile_w > cfg.W ||
+        tile_y + tile_h > cfg.H)
+        return fail(c, PGPU_ERR_INVALID_ARG, "tile %d,%d %dx%d outside the %dx%d image", tile_x,
+                    tile_y, tile_w, tile_h, cfg.W, cfg.H);
+    cfg.count = false;
+    PGPU_CUDA(c, cudaSetDevice(c->device));
+    const bool dev_out = (p->flags & PGPU_FLAG_DEVICE_OUTPUT) != 0;
+    const size_t n3 = (size_t)tile_w * tile_h * 3;
+    float* d_out = out_rgb;
+    if (!dev_out) {
+        if ((rc = ensure(c, c->d_out, c->out_cap, n3 * 4))) return rc;
+        d_out = c->d_out;
+    }
+    const int tile[4] = {tile_x, tile_y, tile_w, tile_h};
+    cudaError_t e = launch_megakernel(ds->view, cfg, d_out, nullptr, c->d_cnt, c->stream, tile);
+    if (e != cudaSuccess) return cuda_fail(c, e, "megakernel launch");
+    if (!dev_out)
+        PGPU_CUDA(c, cudaMemcpyAsync(out_rgb, d_out, n3 * 4, cudaMemcpyDeviceToHost, c->stream));
+    PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     return PGPU_OK;
 }
 

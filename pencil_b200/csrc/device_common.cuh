@@ -107,13 +107,15 @@ __device__ __forceinline__ Ray camera_ray(const float* cam, float u, float v) {
     return Ray{org, normalized(dir)};
 }
 
-// Jittered image-plane point of sample (sx, sy) (src/renderer.hpp:363-366).
+// Jittered image-plane point of sample (sx, sy) (src/renderer.hpp:363-366);
+// `tile`: the distributed worker's jitter of half a pixel
+// (src/distributed.hpp:416-419).
 __device__ __forceinline__ void sample_uv(int i, int j, int sx, int sy, int W, int H, int n,
-                                          Rng& rng, float& u, float& v) {
+                                          Rng& rng, float& u, float& v, bool tile = false) {
     u = (i + (sx + 0.5f) / n) / (float)W;
     v = 1.0f - (j + (sy + 0.5f) / n) / (float)H;
-    u += rng.sym() * (0.5f / (W * n));
-    v += rng.sym() * (0.5f / (H * n));
+    u += rng.sym() * (tile ? 0.5f / W : 0.5f / (W * n));
+    v += rng.sym() * (tile ? 0.5f / H : 0.5f / (H * n));
 }
 
 // Per-ray constants of the slab test. AABB::hit (src/primitives.hpp:38-49)

@@ -28,19 +28,23 @@ mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __re
     Tracer<kMkShared, COUNT> tr{S, P, stk, rc};
 
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long npix = (long long)P.W * P.H;
+    const bool tile = P.tile_w > 0;
+    const int outW = tile ? P.tile_w : P.W, outH = tile ? P.tile_h : P.H;
+    const long long npix = (long long)outW * outH;
     const long long pix = gid / G;
     const int lane_g = (int)(gid % G);
     const bool active = pix < npix;
     V3 acc = v3(0, 0, 0), acc2 = v3(0, 0, 0);
     if (active) {
-        const int i = (int)(pix % P.W), j = (int)(pix / P.W);
+        // pixel of the full image
+        const int i = (int)(pix % outW) + (tile ? P.tile_x : 0);
+        const int j = (int)(pix / outW) + (tile ? P.tile_y : 0);
         if (PIXEL_SEQ) {
             Rng rng{pixel_seed(i, j)};
             for (int sy = 0; sy < P.n; ++sy) {
                 for (int sx = 0; sx < P.n; ++sx) {
                     float u, v;
-                    sample_uv(i, j, sx, sy, P.W, P.H, P.n, rng, u, v);
+                    sample_uv(i, j, sx, sy, P.W, P.H, P.n, rng, u, v, tile);
                     V3 c = tr.template sample<TREE>(camera_ray(S.cam, u, v), rng);
                     acc = acc + c;
                     acc2 = acc2 + c * c;
@@ -50,7 +54,7 @@ mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __re
             for (int s = lane_g; s < P.spp; s += G) {
                 Rng rng{path_seed(i, j, s + P.sample_offset, P.salt)};
                 float u, v;
-                sample_uv(i, j, s % P.n, s / P.n, P.W, P.H, P.n, rng, u, v);
+                sample_uv(i, j, s % P.n, s / P.n, P.W, P.H, P.n, rng, u, v, tile);
                 V3 c = tr.template sample<TREE>(camera_ray(S.cam, u, v), rng);
                 acc = acc + c;
                 acc2 = acc2 + c * c;
@@ -92,7 +96,7 @@ template <bool COUNT, bool TREE, bool PIXEL_SEQ>
 static cudaError_t launch_mk(const SceneView& S, const PathParams& P, int G, float* out,
                              float* m2, unsigned long long* counters, cudaStream_t st) {
     const int block = 128;
-    long long threads = (long long)P.W * P.H * G;
+    long long threads = (P.tile_w > 0 ? (long long)P.tile_w * P.tile_h : (long long)P.W * P.H) * G;
     long long blocks = (threads + block - 1) / block;
     size_t smem = (size_t)kMkShared * block * 8;
     mk_render<COUNT, TREE, PIXEL_SEQ><<<(unsigned)blocks, block, smem, st>>>(S, P, G, out, m2,
@@ -101,9 +105,15 @@ static cudaError_t launch_mk(const SceneView& S, const PathParams& P, int G, flo
 }
 
 cudaError_t launch_megakernel(const SceneView& S, const RenderCfg& c, float* out, float* m2,
-                              unsigned long long* counters, cudaStream_t st) {
+                              unsigned long long* counters, cudaStream_t st, const int* tile) {
     PathParams P{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias, c.salt,
-                 c.sample_offset, c.mis ? 1 : 0};
+                 c.sample_offset, c.mis ? 1 : 0, 0, 0, 0, 0};
+    if (tile) {
+        P.tile_x = tile[0];
+        P.tile_y = tile[1];
+        P.tile_w = tile[2];
+        P.tile_h = tile[3];
+    }
     const bool seq = c.rng == PGPU_RNG_PIXEL_SEQUENTIAL;
     const bool tree = c.glass == PGPU_GLASS_BOTH_BRANCHES;
     int G = 1;

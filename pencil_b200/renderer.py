@@ -158,6 +158,16 @@ class GpuContext:
         del keep
         return nodes[: cnt.value].copy(), depth.value
 
+    def render_tile(self, sid: int, settings: RenderSettings, x: int, y: int, w: int,
+                    h: int) -> np.ndarray:
+        """One tile of the distributed worker (render_tile): settings give the
+        full image; returns (h, w, 3)."""
+        p = settings.params()
+        out = np.empty((h, w, 3), np.float32)
+        self.check(self.lib.pgpu_render_tile(self.h, sid, C.byref(p), x, y, w, h, A.ptr(out)),
+                   "pgpu_render_tile")
+        return out
+
     def scene_info(self, sid: int) -> dict:
         """Sizes of an uploaded scene (device bytes, leaves, binary and wide
         node counts, depth, wide-tree stack need)."""

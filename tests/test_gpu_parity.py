@@ -239,6 +239,29 @@ def test_mis_path_tracing(gpu, seed):
     gpu.free(sid)
 
 
+@pytest.mark.parametrize("seed", [18, 19])
+def test_distributed_worker_tiles(gpu, seed):
+    """pgpu_render_tile against the oracle's render_tile (itself equal to the
+    reference worker's, test_oracle_live_ref.py): Whitted, Pencil's per-pixel
+    RNG; tiles at the corners and inside; tiles cover the image."""
+    from test_oracle_live_ref import random_scene
+    s = random_scene(seed, 60)
+    sid = gpu.upload(s)
+    st = RenderSettings(width=48, height=36, samples=2, max_depth=5, pathtrace=False,
+                        engine=A.ENGINE_MEGAKERNEL, rng=A.RNG_PIXEL_SEQUENTIAL,
+                        glass=A.GLASS_BOTH_BRANCHES)
+    orc = O.Oracle(s)
+    full = np.zeros((36, 48, 3), np.float32)
+    for x, y, w, h in ((0, 0, 24, 18), (24, 0, 24, 18), (0, 18, 24, 18), (24, 18, 24, 18)):
+        t = gpu.render_tile(sid, st, x, y, w, h)
+        near_exact(t, orc.render_tile(st, x, y, w, h))
+        full[y:y + h, x:x + w] = t
+    near_exact(full, orc.render_tile(st, 0, 0, 48, 36))
+    with pytest.raises(A.GpuError):
+        gpu.render_tile(sid, st, 40, 0, 16, 8)
+    gpu.free(sid)
+
+
 @pytest.mark.parametrize("name", ["c1", "cloud2k", "prims_mix", "cornell_box"])
 def test_counter_rng_three_sigma_against_reference(gpu, scenes, name):
     """End to end: GPU production estimator against the reference

@@ -121,6 +121,18 @@ def test_oracle_mis_render_matches_reference(seed):
     assert not np.array_equal(img, plain)        # the weights changed the image
 
 
+@pytest.mark.parametrize("seed", [18, 19])
+def test_oracle_tile_matches_reference_worker(seed):
+    """The distributed worker's render_tile (src/distributed.hpp:380-434):
+    Whitted trace, per-pixel seeds of the full image, half-pixel jitter."""
+    s = random_scene(seed, 60)
+    st = RenderSettings(width=48, height=36, samples=2, max_depth=5, pathtrace=False)
+    for x, y, w, h in ((0, 0, 48, 36), (10, 7, 16, 12), (47, 35, 1, 1)):
+        mine = O.Oracle(s).render_tile(st, x, y, w, h)
+        ref = O.ref_tile(s, 48, 36, x, y, w, h, 2, 5)
+        assert np.array_equal(mine.view(np.uint32), ref.view(np.uint32))
+
+
 @pytest.mark.parametrize("seed", [21, 22])
 def test_oracle_hits_match_reference(seed):
     s = random_scene(seed, 200)
