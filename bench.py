@@ -59,7 +59,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint, batch and image-quality measurements")
-    ap.add_argument("--profile-case", choices=["wavefront", "megakernel"], default=None,
+    ap.add_argument("--profile-case", choices=["wavefront", "megakernel", "adjoint", "lbvh",
+                                               "tonemap"], default=None,
                     help="render the workload once, kernels launched one by one (for ncu)")
     ap.add_argument("--profile-scale", type=int, default=1,
                     help="divide the image width and height by this (smaller ncu cases)")
@@ -565,10 +566,34 @@ class _Null:
 
 
 def run_profile_case(args) -> None:
-    """One frame of the workload with no CUDA graph, for ncu captures."""
+    """One frame of the workload with no CUDA graph, for ncu captures (or one
+    adjoint of the box configuration, one device BVH build of the sphere
+    cloud, one device tonemap of a 1280x720 frame)."""
     from pencil_b200 import _abi as A
     from pencil_b200 import workloads as W
     from pencil_b200.renderer import GpuContext, RenderStats
+    if args.profile_case in ("adjoint", "lbvh", "tonemap"):
+        ctx = GpuContext(0)
+        if args.profile_case == "adjoint":
+            wa, _, _ = W.adjoint_box()
+            sid = ctx.upload(wa.scene)
+            dl = np.random.default_rng(0).normal(
+                size=(wa.settings.height, wa.settings.width, 3)).astype(np.float32)
+            st = RenderStats()
+            ctx.adjoint(sid, wa.settings, dl, wa.scene.n_materials, len(wa.scene.lights), stats=st)
+            out = {"profile_case": "adjoint", "device_ms": st.device_ms}
+            ctx.free(sid)
+        elif args.profile_case == "lbvh":
+            wl = W.sphere_cloud()
+            nodes, depth = ctx.build_bvh_device(wl.scene)
+            out = {"profile_case": "lbvh", "nodes": int(len(nodes)), "depth": depth}
+        else:
+            hdr = np.random.default_rng(1).exponential(0.5, (720, 1280, 3)).astype(np.float32)
+            px = ctx.tonemap(hdr)
+            out = {"profile_case": "tonemap", "bytes": int(px.size)}
+        print(json.dumps(out))
+        ctx.close()
+        return
     wl = W.sphere_cloud()
     st = wl.settings
     st.width //= args.profile_scale

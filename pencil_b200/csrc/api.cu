@@ -47,7 +47,8 @@ cudaError_t launch_adjoint(const SceneView& S, const RenderCfg& c, const float* 
 int adjoint_max_depth();
 int adjoint_max_lights();
 cudaError_t launch_tonemap(const float* d_hdr, long long n_pixels, int mode, float exposure,
-                           uint8_t* d_out, cudaStream_t st);
+                           uint8_t* d_out, const float* d_thr, cudaStream_t st);
+const float* gamma_thresholds_host();
 cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_node>& out,
                         int& depth, cudaStream_t st);
 
@@ -138,6 +139,8 @@ struct pgpu_ctx {
     size_t adj_cap = 0;
     uint8_t* d_rgb8 = nullptr;        // tonemap output staging
     size_t rgb8_cap = 0;
+    float* d_thr = nullptr;           // tonemap gamma thresholds (256 floats)
+    size_t thr_cap = 0;
     // scene arenas come from a stream-ordered pool owned by the context, so
     // that upload / free cycles reuse device memory without cudaMalloc or
     // cudaFree (each of which synchronises the device)
@@ -348,6 +351,7 @@ void pgpu_destroy(pgpu_ctx* c) {
     cudaFree(c->d_query);
     cudaFree(c->d_adj);
     cudaFree(c->d_rgb8);
+    cudaFree(c->d_thr);
     wavefront_delete(c->wf);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -782,7 +786,13 @@ int32_t pgpu_tonemap(pgpu_ctx* c, const float* hdr, int32_t n_pixels, int32_t to
         if (rc) return rc;
         d_dst = c->d_rgb8;
     }
-    PGPU_CUDA(c, launch_tonemap(d_in, n_pixels, tonemap, exposure, d_dst, c->stream));
+    if (!c->d_thr) {
+        int rc = ensure(c, c->d_thr, c->thr_cap, 256 * sizeof(float));
+        if (rc) return rc;
+        PGPU_CUDA(c, cudaMemcpy(c->d_thr, gamma_thresholds_host(), 256 * sizeof(float),
+                                cudaMemcpyHostToDevice));
+    }
+    PGPU_CUDA(c, launch_tonemap(d_in, n_pixels, tonemap, exposure, d_dst, c->d_thr, c->stream));
     if (!(flags & PGPU_TONEMAP_DEVICE_OUTPUT))
         PGPU_CUDA(c, cudaMemcpyAsync(out_rgb8, d_dst, n3, cudaMemcpyDeviceToHost, c->stream));
     PGPU_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -60,9 +60,13 @@ const GammaThresholds& thresholds() {
 
 }  // namespace
 
-// mode: 0 none, 1 ACES, 2 Reinhard (pencil::ToneMap order).
+// mode: 0 none, 1 ACES, 2 Reinhard (pencil::ToneMap order). `thr`: the 256
+// thresholds in device memory, staged in shared memory per block.
 __global__ void tm_rgb8(const float* __restrict__ hdr, long long n3, float e, int mode,
-                        GammaThresholds g, uint8_t* __restrict__ out) {
+                        const float* __restrict__ thr, uint8_t* __restrict__ out) {
+    __shared__ float t[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) t[k] = thr[k];
+    __syncthreads();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3;
          i += (long long)gridDim.x * blockDim.x) {
         float x = hdr[i] * e;
@@ -77,15 +81,18 @@ __global__ void tm_rgb8(const float* __restrict__ hdr, long long n3, float e, in
         int lo = 0, hi = 255;                              // largest k with t[k] <= x
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (g.t[mid] <= x) lo = mid;
+            if (t[mid] <= x) lo = mid;
             else hi = mid - 1;
         }
         out[i] = (uint8_t)lo;
     }
 }
 
+// The 256 thresholds (t[0] unused) for upload to the device.
+const float* gamma_thresholds_host() { return thresholds().t; }
+
 cudaError_t launch_tonemap(const float* d_hdr, long long n_pixels, int mode, float exposure,
-                           uint8_t* d_out, cudaStream_t st) {
+                           uint8_t* d_out, const float* d_thr, cudaStream_t st) {
     const float e = std::pow(2.0f, exposure);             // tonemap_color's exposure
     const long long n3 = 3 * n_pixels;
     int dev = 0, sms = 0;
@@ -93,7 +100,7 @@ cudaError_t launch_tonemap(const float* d_hdr, long long n_pixels, int mode, flo
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long blocks = (n3 + 255) / 256;
     const int grid = (int)(blocks < (long long)sms * 16 ? (blocks > 0 ? blocks : 1) : sms * 16);
-    tm_rgb8<<<grid, 256, 0, st>>>(d_hdr, n3, e, mode, thresholds(), d_out);
+    tm_rgb8<<<grid, 256, 0, st>>>(d_hdr, n3, e, mode, d_thr, d_out);
     return cudaGetLastError();
 }
 
