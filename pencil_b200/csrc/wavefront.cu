@@ -374,26 +374,23 @@ __global__ void __launch_bounds__(kWfBlock) wf_extend_packet(WfArgs A) {
                     key[k] = __uint_as_float(__reduce_min_sync(
                         0xffffffffu, reach ? __float_as_uint(ee[k]) : 0x7f800000u));
                 }
-                auto cs = [&](int a, int b) {
-                    if (key[b] < key[a]) {
-                        const float tk = key[a]; key[a] = key[b]; key[b] = tk;
-                        const int tr2 = ref[a]; ref[a] = ref[b]; ref[b] = tr2;
-                    }
-                };
-                cs(0, 1); cs(2, 3); cs(0, 2); cs(1, 3); cs(1, 2);
-                if (key[0] != INFINITY) {
-                    __syncwarp();
-                    if (lane == 0) {
+                // the nearest child next; the others stacked in child order
+                // (a full sort of four keys cost more than it saved)
+                int best = 0;
+                float kb = key[0];
 #pragma unroll
-                        for (int k = 3; k >= 1; --k)
-                            if (key[k] != INFINITY) { sref[sp] = ref[k]; skey[sp] = key[k]; ++sp; }
-                    } else {
-#pragma unroll
-                        for (int k = 3; k >= 1; --k)
-                            if (key[k] != INFINITY) ++sp;
-                    }
+                for (int k = 1; k < 4; ++k)
+                    if (key[k] < kb) { kb = key[k]; best = k; }
+                if (kb != INFINITY) {
                     __syncwarp();
-                    node = ref[0];
+#pragma unroll
+                    for (int k = 3; k >= 0; --k)
+                        if (k != best && key[k] != INFINITY) {
+                            if (lane == 0) { sref[sp] = ref[k]; skey[sp] = key[k]; }
+                            ++sp;
+                        }
+                    __syncwarp();
+                    node = best == 0 ? ref[0] : best == 1 ? ref[1] : best == 2 ? ref[2] : ref[3];
                     continue;
                 }
                 // pop the nearest entry some lane may still reach
