@@ -235,8 +235,9 @@ typedef struct pgpu_render_params {
                                    most this many of its 32 lanes are still
                                    traversing (0: automatic)                 */
     int32_t  sort_key;          /* wavefront ray order: 0 queue order, 1 binned
-                                   by direction octant, 2 sorted by origin
-                                   (Morton code) and direction octant        */
+                                   by direction octant, 2 shadow work sorted
+                                   by origin (Morton code) and octant, 3 also
+                                   the extension rays of bounces >= 1        */
 } pgpu_render_params;
 
 typedef struct pgpu_stats {

@@ -8,7 +8,8 @@ workload (image size, samples, scene, light count) and the GPU:
   refill_below    a warp of the persistent traversal kernels fetches new rays
                   once at most this many of its lanes are still traversing
   sort_key        0: queue order; 1: rays binned by direction octant;
-                  2: rays (and shadow work) sorted by origin cell and octant
+                  2: shadow work sorted by origin cell and octant; 3: also the
+                  extension rays after the first bounce
 
 `autotune` times candidates with short device-resident renders (CUDA events
 on the render stream, a warm-up render first) by coordinate search: capacity
@@ -32,7 +33,7 @@ CACHE = Path(os.environ.get("PGPU_AUTOTUNE_CACHE",
 
 CAPACITIES = (1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24)
 REFILLS = (12, 16, 20, 24)
-SORT_KEYS = (0, 1, 2)
+SORT_KEYS = (0, 1, 2, 3)
 
 
 def signature(scene, settings_list: list[RenderSettings]) -> str:

@@ -873,8 +873,8 @@ int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, Re
         return fail(c, PGPU_ERR_INVALID_ARG, "refill_below must be 0..31");
     cfg.refill = p->refill_below;
     cfg.queue_capacity = p->queue_capacity;
-    if (p->sort_key < 0 || p->sort_key > 2)
-        return fail(c, PGPU_ERR_INVALID_ARG, "sort_key must be 0, 1 or 2");
+    if (p->sort_key < 0 || p->sort_key > 3)
+        return fail(c, PGPU_ERR_INVALID_ARG, "sort_key must be 0..3");
     cfg.sort_key = p->sort_key;
     cfg.profile = (p->flags & PGPU_FLAG_PROFILE_KERNELS) != 0;
     cfg.packets = (p->flags & PGPU_FLAG_NO_PACKETS) == 0;

@@ -84,13 +84,19 @@ struct WfArgs {
     int packets;              // 1: the first bounce of a one-scene frame as warp packets
     int refill_below;         // extend/shadow: a warp refetches rays once at most
                               // this many of its lanes are still traversing
-    // sort key 2 (counting sort of each iteration's shadow work by sort_key_of):
+    // sort keys 2/3 (counting sort by sort_key_of of each iteration's shadow
+    // work, and with key 3 of its next extension rays):
     int* key_s;               // [slot] key of the slot's first shadow ray
     int* tmp_s;               // unsorted slots with shadow work
     int* qs;                  // the same slots sorted by key
     int* hist_s;              // kSortBins counters, then local bin offsets
     int* chunk_off;           // kSortBins / 1024 chunk totals, then chunk offsets
     int* tcnt;                // [iteration * 2 + 1] slots with shadow work
+    int* key_e;               // [slot] key of the path's next extension ray
+    int* qe;                  // the next queue sorted by key (shade keeps the
+                              // unsorted one: it reads path state by slot)
+    int* hist_e;
+    int* chunk_off_e;
 };
 
 // Sort key of a ray: Morton code of its origin in the scene's root box
@@ -258,6 +264,7 @@ wf_extend(WfArgs A, int it) {
     stk.stride = blockDim.x;
     RayCount rc = {};
     const QView qv = qview(A, it);
+    const bool sorted_e = A.sort_key == 3 && it > 0;   // shade sorted this queue too
     unsigned int* cursor = A.work + it * 3 + 0;
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
@@ -277,7 +284,7 @@ wf_extend(WfArgs A, int it) {
             if (!active) {
                 const int e = base + __popc(idle & below);
                 if (e < qv.total) {
-                    slot = qv.slot(e);
+                    slot = sorted_e ? A.qe[e] : qv.slot(e);
                     S = &A.views[A.jobs[A.st[slot].w].view];
                     const float4 o = A.ray_o[slot], d = A.ray_d[slot];
                     if (COUNT) rc.ext++;
@@ -466,6 +473,7 @@ wf_shade(WfArgs A, int it) {
         int slot = -1;
         int bin = 0;
         int key = -1;
+        int key_next = -1;
         if (e < qv.total) {
             slot = qv.slot(e);
             uint4 stv = A.st[slot];
@@ -488,7 +496,7 @@ wf_shade(WfArgs A, int it) {
             alive = shade_vertex(S, J.P, ps, found, h, E);
             E.store();
             shadow_work = E.kind != 0;
-            if (A.sort_key == 2 && shadow_work) {
+            if (A.sort_key >= 2 && shadow_work) {
                 key = sort_key_of(S, E.o0, E.d0);
                 A.key_s[slot] = key;
             }
@@ -502,15 +510,23 @@ wf_shade(WfArgs A, int it) {
                 if (A.sort_key == 1)
                     bin = (ps.ray.d.x < 0.0f ? 1 : 0) | (ps.ray.d.y < 0.0f ? 2 : 0) |
                           (ps.ray.d.z < 0.0f ? 4 : 0);
+                if (A.sort_key == 3) {
+                    key_next = sort_key_of(S, ps.ray.o, ps.ray.d);
+                    A.key_e[slot] = key_next;
+                }
             }
         }
         // sort key 2: the unsorted list of slots with shadow work, ordered by
         // wf_sort_scatter
-        if (A.sort_key == 2) {
+        if (A.sort_key >= 2) {
             warp_append(shadow_work, slot, A.tcnt + 2 * it + 1, A.tmp_s, lane);
             // bin counts, one atomic per distinct key in the warp
             const unsigned same = __match_any_sync(0xffffffffu, key);
             if (shadow_work && lane == __ffs(same) - 1) atomicAdd(A.hist_s + key, __popc(same));
+        }
+        if (A.sort_key == 3) {
+            const unsigned same = __match_any_sync(0xffffffffu, key_next);
+            if (alive && lane == __ffs(same) - 1) atomicAdd(A.hist_e + key_next, __popc(same));
         }
         // warp-aggregated append, one atomic per (warp, bin)
         const int nbins = A.sort_key == 1 ? kOctants : 1;
@@ -561,16 +577,16 @@ __device__ __forceinline__ int block_scan_1024(int v, int* s_warp, int* total) {
     return x - v + (warp ? s_warp[warp - 1] : 0);
 }
 
-__global__ void __launch_bounds__(kSortChunk) wf_sort_scan(WfArgs A) {
+__global__ void __launch_bounds__(kSortChunk) wf_sort_scan(int* hist, int* chunk_off) {
     __shared__ int s_warp[32];
-    int* h = A.hist_s + (size_t)blockIdx.x * kSortChunk;
+    int* h = hist + (size_t)blockIdx.x * kSortChunk;
     int total = 0;
     const int ex = block_scan_1024(h[threadIdx.x], s_warp, &total);
     h[threadIdx.x] = ex;
-    if (threadIdx.x == 0) A.chunk_off[blockIdx.x] = total;
+    if (threadIdx.x == 0) chunk_off[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(kSortChunk) wf_sort_chunks(WfArgs A) {
+__global__ void __launch_bounds__(kSortChunk) wf_sort_chunks(int* chunk_off) {
     __shared__ int s_warp[32];
     constexpr int per = (kSortChunks + kSortChunk - 1) / kSortChunk;
     int v[per];
@@ -578,7 +594,7 @@ __global__ void __launch_bounds__(kSortChunk) wf_sort_chunks(WfArgs A) {
 #pragma unroll
     for (int k = 0; k < per; ++k) {
         const int c = threadIdx.x * per + k;
-        v[k] = c < kSortChunks ? A.chunk_off[c] : 0;
+        v[k] = c < kSortChunks ? chunk_off[c] : 0;
         sum += v[k];
     }
     int total = 0;
@@ -586,30 +602,33 @@ __global__ void __launch_bounds__(kSortChunk) wf_sort_chunks(WfArgs A) {
 #pragma unroll
     for (int k = 0; k < per; ++k) {
         const int c = threadIdx.x * per + k;
-        if (c < kSortChunks) A.chunk_off[c] = run;
+        if (c < kSortChunks) chunk_off[c] = run;
         run += v[k];
     }
 }
 
 // Places every listed slot at its bin's next position (the order inside a
 // bin is arbitrary; a path's result does not depend on its queue position).
-__global__ void __launch_bounds__(kWfBlock) wf_sort_scatter(WfArgs A, int it) {
-    const int ns = A.tcnt[2 * it + 1];
+// list[0, *count) -> out by key[slot].
+__global__ void __launch_bounds__(kWfBlock)
+wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
+                const int* chunk_off, int* out) {
+    const int ns = *count;
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;
     // whole warps iterate together (the key match below needs every lane)
     for (int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); e0 < ns; e0 += stride) {
         const int e = e0 + lane;
         const bool on = e < ns;
-        const int slot = on ? A.tmp_s[e] : -1;
-        const int key = on ? A.key_s[slot] : -1;
+        const int slot = on ? list[e] : -1;
+        const int key = on ? keyof[slot] : -1;
         const unsigned same = __match_any_sync(0xffffffffu, key);
         const int leader = __ffs(same) - 1;
         int base = 0;
         if (on && lane == leader)
-            base = A.chunk_off[key / kSortChunk] + atomicAdd(A.hist_s + key, __popc(same));
+            base = chunk_off[key / kSortChunk] + atomicAdd(hist + key, __popc(same));
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (on) A.qs[base + __popc(same & ((1u << lane) - 1u))] = slot;
+        if (on) out[base + __popc(same & ((1u << lane) - 1u))] = slot;
     }
 }
 
@@ -629,7 +648,7 @@ wf_shadow(WfArgs A, int it) {
     RayCount rc = {};
     const QView qv = qview(A, it);
     // sort key 2: the slots with shadow work, sorted by their first shadow ray
-    const bool sorted = A.sort_key == 2;
+    const bool sorted = A.sort_key >= 2;
     const int total = sorted ? A.tcnt[2 * it + 1] : qv.total;
     unsigned int* cursor = A.work + it * 3 + 2;
     const int lane = threadIdx.x & 31;
@@ -804,9 +823,9 @@ static cudaError_t ensure_scratch(WfScratch& W, int Q, int maxS, int iters, int 
     sz += al((size_t)(iters + 2) * kOctants * 4);    // counts
     sz += al((size_t)(iters + 2) * 3 * 4);           // work cursors
     sz += al(4);                                     // status
-    sz += 3 * al((size_t)Q * 4);                     // sort: keys, list, shadow queue
-    sz += al((size_t)kSortBins * 4);                 // sort: bin histogram
-    sz += al((size_t)kSortChunks * 4);               // sort: chunk offsets
+    sz += 5 * al((size_t)Q * 4);                     // sort: keys, list, sorted queues
+    sz += 2 * al((size_t)kSortBins * 4);             // sort: bin histograms
+    sz += 2 * al((size_t)kSortChunks * 4);           // sort: chunk offsets
     sz += al((size_t)(iters + 2) * 2 * 4);           // sort: list counts
     sz += al((size_t)n_views * sizeof(SceneView));
     sz += al((size_t)n_jobs * sizeof(WfJob));
@@ -845,6 +864,10 @@ static cudaError_t ensure_scratch(WfScratch& W, int Q, int maxS, int iters, int 
     A.qs = reinterpret_cast<int*>(take((size_t)Q * 4));
     A.hist_s = reinterpret_cast<int*>(take((size_t)kSortBins * 4));
     A.chunk_off = reinterpret_cast<int*>(take((size_t)kSortChunks * 4));
+    A.key_e = reinterpret_cast<int*>(take((size_t)Q * 4));
+    A.qe = reinterpret_cast<int*>(take((size_t)Q * 4));
+    A.hist_e = reinterpret_cast<int*>(take((size_t)kSortBins * 4));
+    A.chunk_off_e = reinterpret_cast<int*>(take((size_t)kSortChunks * 4));
     A.tcnt = reinterpret_cast<int*>(take((size_t)(iters + 2) * 2 * 4));
     W.d_views = reinterpret_cast<SceneView*>(take((size_t)n_views * sizeof(SceneView)));
     W.d_jobs = reinterpret_cast<WfJob*>(take((size_t)n_jobs * sizeof(WfJob)));
@@ -951,7 +974,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         size_t cnt_bytes = (size_t)(iters + 2) * kOctants * 4;
         if ((e = cudaMemsetAsync(A.counts, 0, cnt_bytes, st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(A.work, 0, (size_t)(iters + 2) * 3 * 4, st)) != cudaSuccess) return e;
-        if (A.sort_key == 2 &&
+        if (A.sort_key >= 2 &&
             (e = cudaMemsetAsync(A.tcnt, 0, (size_t)(iters + 2) * 2 * 4, st)) != cudaSuccess)
             return e;
         int gblocks = (int)((slots + kWfBlock - 1) / kWfBlock);
@@ -967,15 +990,29 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
                 wf_extend<COUNT><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
             lt.mark(KC_EXTEND, st, false);
             lt.mark(KC_SHADE, st, true);
-            if (A.sort_key == 2) {
+            if (A.sort_key >= 2) {
                 if ((e = cudaMemsetAsync(A.hist_s, 0, (size_t)kSortBins * 4, st)) != cudaSuccess)
                     return e;
             }
+            const bool sort_next = A.sort_key == 3 && it + 1 < iters;
+            if (sort_next &&
+                (e = cudaMemsetAsync(A.hist_e, 0, (size_t)kSortBins * 4, st)) != cudaSuccess)
+                return e;
             wf_shade<COUNT><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
-            if (A.sort_key == 2) {
-                wf_sort_scan<<<kSortChunks, kSortChunk, 0, st>>>(A);
-                wf_sort_chunks<<<1, kSortChunk, 0, st>>>(A);
-                wf_sort_scatter<<<occ.grid_scatter, kWfBlock, 0, st>>>(A, it);
+            if (A.sort_key >= 2) {
+                wf_sort_scan<<<kSortChunks, kSortChunk, 0, st>>>(A.hist_s, A.chunk_off);
+                wf_sort_chunks<<<1, kSortChunk, 0, st>>>(A.chunk_off);
+                wf_sort_scatter<<<occ.grid_scatter, kWfBlock, 0, st>>>(
+                    A.tmp_s, A.tcnt + 2 * it + 1, A.key_s, A.hist_s, A.chunk_off, A.qs);
+                n_launch += 3;
+            }
+            if (sort_next) {
+                // the survivors shade just queued (unsorted) -> qe in key order
+                wf_sort_scan<<<kSortChunks, kSortChunk, 0, st>>>(A.hist_e, A.chunk_off_e);
+                wf_sort_chunks<<<1, kSortChunk, 0, st>>>(A.chunk_off_e);
+                wf_sort_scatter<<<occ.grid_scatter, kWfBlock, 0, st>>>(
+                    A.q[(it + 1) & 1], A.counts + (it + 1) * kOctants, A.key_e, A.hist_e,
+                    A.chunk_off_e, A.qe);
                 n_launch += 3;
             }
             lt.mark(KC_SHADE, st, false);

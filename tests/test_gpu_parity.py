@@ -189,9 +189,9 @@ def test_wavefront_equals_megakernel(gpu, scenes, name, mode):
     wf = gpu.render(sid, st, stats=s2)
     assert np.array_equal(mk.view(np.uint32), wf.view(np.uint32))
     assert (s1.extension_rays, s1.shadow_rays) == (s2.extension_rays, s2.shadow_rays)
-    for key in (1, 2):          # octant bins; origin/octant counting sort
+    for key in (1, 2, 3):       # octant bins; origin/octant counting sorts
         st.sort_key = key
-        st.queue_capacity = 4096 if key == 2 else 0   # several chunks
+        st.queue_capacity = 4096 if key >= 2 else 0   # several chunks
         wf2 = gpu.render(sid, st)
         assert np.array_equal(mk.view(np.uint32), wf2.view(np.uint32)), key
 
@@ -304,11 +304,12 @@ def test_batch_equals_individual_renders(gpu):
     batch = gpu.render_batch(sids, sts)
     for a, b in zip(singles, batch):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
-    for st in sts:                 # scenes of a batch share the sort bins
-        st.sort_key = 2
-    batch = gpu.render_batch(sids, sts)
-    for a, b in zip(singles, batch):
-        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    for key in (2, 3):             # scenes of a batch share the sort bins
+        for st in sts:
+            st.sort_key = key
+        batch = gpu.render_batch(sids, sts)
+        for a, b in zip(singles, batch):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     for s in sids:
         gpu.free(s)
 
@@ -374,7 +375,7 @@ def test_invalid_arguments_return_status(gpu):
     sid = gpu.upload(s)
     bad = [RenderSettings(width=0, height=4), RenderSettings(width=4, height=4, samples=0),
            RenderSettings(width=4, height=4, samples=100),
-           RenderSettings(width=4, height=4, sort_key=3)]
+           RenderSettings(width=4, height=4, sort_key=4)]
     for st in bad:
         with pytest.raises(A.GpuError) as e:
             gpu.render(sid, st)
