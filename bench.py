@@ -531,8 +531,11 @@ def measure_mesh(ctx, stream) -> dict:
     upload_ms = (time.perf_counter() - t0) * 1e3
     info = ctx.scene_info(sm)
     st = wm.settings
-    st.queue_capacity, st.refill_below, st.sort_key = 1 << 24, 16, 2
     paths = st.width * st.height * st.samples ** 2
+    # launch parameters for this workload from the autotuner (its capacity
+    # candidates stop at 16M paths, several chunks of this frame)
+    from pencil_b200.autotune import autotune
+    tuned = autotune(ctx, [sm], [st], scene=wm.scene, reps=1, use_cache=False)
     buf = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")
     st.engine = A.ENGINE_WAVEFRONT
     wf_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 2)
@@ -553,8 +556,8 @@ def measure_mesh(ctx, stream) -> dict:
             "wavefront_mrays_s": rays / wf_ms / 1e3,
             "megakernel_ms": mk_ms, "megakernel_mpaths_s": paths / mk_ms / 1e3,
             "wavefront_over_megakernel": mk_ms / wf_ms,
-            "settings": {"queue_capacity": st.queue_capacity, "refill_below": st.refill_below,
-                         "sort_key": st.sort_key}}
+            "autotuned": {k: tuned[k] for k in ("queue_capacity", "refill_below", "sort_key",
+                                                 "ms")}}
 
 
 class _Null:

@@ -69,9 +69,9 @@ struct WfArgs {
     float4* L;
     uint4* st;                // rng, depth, flags, job
     float4* hit;              // t, best ref, leaf slot, found
-    float4* pb;               // pending base.xyz, record count
-    float4* pt;               // pending tail.xyz, scale s
-    float4* pw;               // pending weight.xyz, kind
+    float4* pb;               // Whitted vertex: pending base.xyz, scale s
+    float4* pt;               // pending tail.xyz, kind | shadow records << 2
+    float4* pw;               // Whitted vertex: pending weight.xyz
     float4* sh_o;             // [k * Q + slot] origin.xyz, tmin
     float4* sh_d;             // direction.xyz, tmax
     float4* sh_c;             // contribution.xyz, test | group_end << 1
@@ -233,7 +233,7 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
         A.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
         A.T[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
         A.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        A.pw[slot] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
+        A.pt[slot] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));   // nothing pending
         uint32_t flags = P.mode == kModeWhitted ? kFlagWhitted : 0u;
         A.st[slot] = make_uint4(rng.s, (unsigned)P.depth, flags, (unsigned)jb);
         if (COUNT) rc.ref++;
@@ -449,9 +449,13 @@ struct StoreNee {
     }
     __device__ __forceinline__ void pending(V3 tl, V3 ww, float ss) { tail = tl; w = ww; s = ss; }
     __device__ __forceinline__ void store() {
-        A.pb[slot] = make_float4(base.x, base.y, base.z, __int_as_float(n));
-        A.pt[slot] = make_float4(tail.x, tail.y, tail.z, s);
-        A.pw[slot] = make_float4(w.x, w.y, w.z, __int_as_float(kind));
+        // pt: tail and kind | records << 2; a Whitted vertex also needs its
+        // base and scale (pb) and weight (pw)
+        A.pt[slot] = make_float4(tail.x, tail.y, tail.z, __int_as_float(kind | (n << 2)));
+        if (kind == 2) {
+            A.pb[slot] = make_float4(base.x, base.y, base.z, s);
+            A.pw[slot] = make_float4(w.x, w.y, w.z, 0.0f);
+        }
     }
 };
 
@@ -682,8 +686,15 @@ wf_shadow(WfArgs A, int it) {
             }
             ++k;
         }
-        const float4 pt = A.pt[slot], pw = A.pw[slot];
-        acc.finish(L, v3(pt.x, pt.y, pt.z), v3(pw.x, pw.y, pw.z), pt.w);
+        const float4 pt = A.pt[slot];
+        V3 w = v3(0.0f, 0.0f, 0.0f);
+        float sc = 0.0f;
+        if (acc.kind == 2) {
+            const float4 pw = A.pw[slot];
+            w = v3(pw.x, pw.y, pw.z);
+            sc = A.pb[slot].w;
+        }
+        acc.finish(L, v3(pt.x, pt.y, pt.z), w, sc);
         A.L[slot] = make_float4(L.x, L.y, L.z, 0.0f);
         return false;
     };
@@ -700,14 +711,19 @@ wf_shadow(WfArgs A, int it) {
                 const int e = base + __popc(idle & below);
                 if (e < total) {
                     slot = sorted ? A.qs[e] : qv.slot(e);
-                    const int kind = __float_as_int(A.pw[slot].w);
+                    const int info = __float_as_int(A.pt[slot].w);
+                    const int kind = info & 3;
                     if (kind != 0) {
                         S = &A.views[A.jobs[A.st[slot].w].view];
-                        const float4 pb = A.pb[slot], L4 = A.L[slot];
-                        if (kind == 1) acc.begin_pt();
-                        else acc.begin_whitted(v3(pb.x, pb.y, pb.z));
+                        const float4 L4 = A.L[slot];
+                        if (kind == 1) {
+                            acc.begin_pt();
+                        } else {
+                            const float4 pb = A.pb[slot];
+                            acc.begin_whitted(v3(pb.x, pb.y, pb.z));
+                        }
                         L = v3(L4.x, L4.y, L4.z);
-                        n = __float_as_int(pb.w);
+                        n = info >> 2;
                         k = 0;
                         active = advance();
                     }
