@@ -56,8 +56,9 @@ constexpr int kMaxDepth = 64;          // traversal stack bound (kMaxStack)
 constexpr int kMaxTreeFrames = 32;     // Whitted recursion bound of the two-branch mode
 
 struct DeviceScene {
-    void* arena = nullptr;
-    size_t bytes = 0;
+    void* arena = nullptr;             // binary nodes, leaves, vertices, materials, lights
+    void* arena_wide = nullptr;        // 4-wide nodes (null when the root is a leaf)
+    size_t bytes = 0;                  // both arenas
     SceneView view{};
     int n_unified = 0;
     int n_leaves = 0;
@@ -147,7 +148,9 @@ struct pgpu_ctx {
     cudaMemPool_t pool = nullptr;
     // host workspace of uploads, kept between calls (no page faults on reuse)
     std::vector<int> ws_idx, ws_leaf_ref;
-    std::vector<float4> ws_wide;
+    std::vector<int2> ws_size_height;
+    std::vector<char> ws_seen;
+    WideScratch ws_collapse;
     std::vector<DevMaterial> spare_mats;   // material table of the last freed scene
 };
 
@@ -256,40 +259,39 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     if (n_nodes != 2 * n_prims - 1)
         return fail(c, PGPU_ERR_BVH_INVALID, "%d nodes for %d primitives (need 2n-1)", n_nodes,
                     n_prims);
+    {
+        const int bad = first_bad(n_nodes, [&](int k) {
+            return !finite3(nodes[k].bmin) || !finite3(nodes[k].bmax);
+        });
+        if (bad >= 0) return fail(c, PGPU_ERR_BVH_INVALID, "node %d has a non-finite box", bad);
+    }
     // DFS pre-order (the order Pencil's recursive build emits): an interior
     // node k has its left subtree at k + 1 and its right subtree right after
-    // the left one. Subtree sizes, from the back, check exactly that.
-    std::vector<int> size(n_nodes);
+    // the left one. Subtree sizes, from the back, check exactly that; the
+    // same sweep takes subtree heights (the root's is the depth) and checks
+    // that every primitive is in exactly one leaf.
+    std::vector<int2>& sh = c->ws_size_height;     // (subtree size, height)
+    sh.resize(n_nodes);
+    std::vector<char>& seen = c->ws_seen;
+    seen.assign(n_prims, 0);
     for (int k = n_nodes - 1; k >= 0; --k) {
         const pgpu_bvh_node& nd = nodes[k];
-        if (!finite3(nd.bmin) || !finite3(nd.bmax))
-            return fail(c, PGPU_ERR_BVH_INVALID, "node %d has a non-finite box", k);
         if (nd.left < 0) {
             if (nd.right < 0 || nd.right >= n_prims)
                 return fail(c, PGPU_ERR_BVH_INVALID, "leaf %d references primitive %d", k, nd.right);
-            size[k] = 1;
+            if (seen[nd.right]++)
+                return fail(c, PGPU_ERR_BVH_INVALID, "primitive %d is in two leaves", nd.right);
+            sh[k] = make_int2(1, 1);
             continue;
         }
         if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes ||
-            nd.right != nd.left + size[nd.left])
+            nd.right != nd.left + sh[nd.left].x)
             return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
-        size[k] = 1 + size[nd.left] + size[nd.right];
+        sh[k] = make_int2(1 + sh[nd.left].x + sh[nd.right].x,
+                          1 + std::max(sh[nd.left].y, sh[nd.right].y));
     }
-    if (size[0] != n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "unreachable nodes in table");
-    // every primitive in exactly one leaf; levels
-    std::vector<int> level(n_nodes);
-    std::vector<char> seen_prim(n_prims, 0);
-    level[0] = 1;
-    for (int k = 0; k < n_nodes; ++k) {
-        const pgpu_bvh_node& nd = nodes[k];
-        depth = std::max(depth, level[k]);
-        if (nd.left < 0) {
-            if (seen_prim[nd.right]++)
-                return fail(c, PGPU_ERR_BVH_INVALID, "primitive %d is in two leaves", nd.right);
-        } else {
-            level[nd.left] = level[nd.right] = level[k] + 1;
-        }
-    }
+    if (sh[0].x != n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "unreachable nodes in table");
+    depth = sh[0].y;
     if (depth > kMaxDepth)
         return fail(c, PGPU_ERR_UNSUPPORTED, "BVH depth %d exceeds %d", depth, kMaxDepth);
     return PGPU_OK;
@@ -341,7 +343,10 @@ void pgpu_destroy(pgpu_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (auto& kv : c->scenes) cudaFreeAsync(kv.second->arena, c->stream);
+    for (auto& kv : c->scenes) {
+        cudaFreeAsync(kv.second->arena, c->stream);
+        if (kv.second->arena_wide) cudaFreeAsync(kv.second->arena_wide, c->stream);
+    }
     c->scenes.clear();
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->pool) cudaMemPoolDestroy(c->pool);
@@ -461,18 +466,29 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         });
         if (bad >= 0) return check_prim(c, s->prims[bad], bad, s->n_materials);
     }
-    for (int k = 0; k < s->n_mesh_triangles; ++k) {
-        for (int v = 0; v < 3; ++v) {
-            int idx = s->mesh_indices[3 * k + v];
-            if (idx < 0 || idx >= s->n_mesh_vertices)
-                return fail(c, PGPU_ERR_INVALID_ARG, "mesh triangle %d vertex %d out of range", k, idx);
+    {
+        const int bad = first_bad(s->n_mesh_triangles, [&](int k) {
+            for (int v = 0; v < 3; ++v) {
+                const int idx = s->mesh_indices[3 * k + v];
+                if (idx < 0 || idx >= s->n_mesh_vertices) return true;
+            }
+            return s->mesh_materials[k] < 0 || s->mesh_materials[k] >= s->n_materials;
+        });
+        if (bad >= 0) {
+            for (int v = 0; v < 3; ++v) {
+                const int idx = s->mesh_indices[3 * bad + v];
+                if (idx < 0 || idx >= s->n_mesh_vertices)
+                    return fail(c, PGPU_ERR_INVALID_ARG, "mesh triangle %d vertex %d out of range",
+                                bad, idx);
+            }
+            return fail(c, PGPU_ERR_INVALID_ARG, "mesh triangle %d material out of range", bad);
         }
-        if (s->mesh_materials[k] < 0 || s->mesh_materials[k] >= s->n_materials)
-            return fail(c, PGPU_ERR_INVALID_ARG, "mesh triangle %d material out of range", k);
     }
-    for (int k = 0; k < s->n_mesh_vertices; ++k)
-        if (!finite3(s->mesh_vertices + 3 * k))
-            return fail(c, PGPU_ERR_INVALID_ARG, "mesh vertex %d is not finite", k);
+    {
+        const int bad = first_bad(s->n_mesh_vertices,
+                                  [&](int k) { return !finite3(s->mesh_vertices + 3 * k); });
+        if (bad >= 0) return fail(c, PGPU_ERR_INVALID_ARG, "mesh vertex %d is not finite", bad);
+    }
     {
         const int bad = first_bad(s->n_materials, [&](int k) {
             const pgpu_material& m = s->materials[k];
@@ -484,24 +500,6 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
             return fail(c, PGPU_ERR_UNSUPPORTED, "material %d has unsupported kind %d", bad, m.kind);
         }
     }
-    std::vector<DevMaterial> mats = std::move(c->spare_mats);   // pages already mapped
-    c->spare_mats = {};
-    mats.resize(s->n_materials);
-    parallel_for(s->n_materials, [&](int b, int e) {
-        for (int k = b; k < e; ++k) {
-            const pgpu_material& m = s->materials[k];
-            DevMaterial d{};
-            std::memcpy(d.albedo, m.albedo, 12);
-            d.kind = m.kind;
-            std::memcpy(d.emission, m.emission, 12);
-            d.reflectivity = m.reflectivity;
-            d.ior = m.ior;
-            d.specular = m.specular;
-            d.shininess = m.shininess;
-            std::memcpy(d.specular_color, m.specular_color, 12);
-            mats[k] = d;
-        }
-    });
     std::vector<DevLight> lights(s->n_lights);
     std::vector<int> quad_mats;
     int has_quad = 0;
@@ -523,7 +521,6 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
             HV cr = hcross(hv(l.edge_u), hv(l.edge_v));
             d.area = std::sqrt(cr.x * cr.x + cr.y * cr.y + cr.z * cr.z);
             if (!(d.area > 0.0f)) return fail(c, PGPU_ERR_INVALID_ARG, "quad light %d has no area", k);
-            mats[l.material].area_emitter = 1;
             quad_mats.push_back(l.material);
             has_quad = 1;
         }
@@ -561,51 +558,41 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         int type = prim < s->n_prims ? s->prims[prim].type : PGPU_PRIM_TRIANGLE;
         return ~((type << kLeafTypeShift) | idx[k]);
     };
-    // 4-wide nodes for the wavefront's traversal
-    std::vector<int>& leaf_ref = c->ws_leaf_ref;
-    leaf_ref.resize(n_nodes);
-    parallel_for(n_nodes, [&](int b, int e) {
-        for (int k = b; k < e; ++k) leaf_ref[k] = nodes[k].left < 0 ? ref_of(k) : 0;
-    });
-    std::vector<float4>& wide = c->ws_wide;
-    int wide_stack = 0;
-    const int n_wide = collapse_wide(nodes, n_nodes, leaf_ref, kMaxDepth, wide, wide_stack);
-    if (wide_stack > kMaxDepth)
-        return fail(c, PGPU_ERR_UNSUPPORTED, "BVH needs %d stack entries, more than %d",
-                    wide_stack, kMaxDepth);
 
+    // Staging: the main arena's bytes, then room for one wide node per
+    // binary interior node (the most the collapse can make). The main part
+    // is copied to the device while the wide nodes are being built.
     size_t off_nodes = 0;
-    size_t off_wide = align256(off_nodes + (size_t)n_int * 64);
-    size_t off_ga = align256(off_wide + (size_t)n_wide * kWideNodeFloat4 * 16);
+    size_t off_ga = align256(off_nodes + (size_t)n_int * 64);
     size_t off_gb = align256(off_ga + (size_t)n_leaf * 16);
     size_t off_vt = align256(off_gb + (size_t)n_leaf * 16);
     size_t off_lm = align256(off_vt + n_verts * 16);
     size_t off_lp = align256(off_lm + (size_t)n_leaf * 4);
     size_t off_mt = align256(off_lp + (size_t)n_leaf * 4);
-    size_t off_lt = align256(off_mt + mats.size() * sizeof(DevMaterial));
+    size_t off_lt = align256(off_mt + (size_t)s->n_materials * sizeof(DevMaterial));
     size_t total = align256(off_lt + lights.size() * sizeof(DevLight));
-    if (c->stage_cap < total) {
+    const size_t wide_cap = (size_t)n_int * kWideNodeFloat4 * 16;
+    if (c->stage_cap < total + wide_cap) {
         if (c->h_stage) cudaFreeHost(c->h_stage);
         c->h_stage = nullptr;
         c->stage_cap = 0;
-        if (cudaMallocHost(reinterpret_cast<void**>(&c->h_stage), total) != cudaSuccess) {
+        if (cudaMallocHost(reinterpret_cast<void**>(&c->h_stage), total + wide_cap) != cudaSuccess) {
             c->h_stage = nullptr;
-            return fail(c, PGPU_ERR_OUT_OF_MEMORY, "pinned staging of %zu bytes", total);
+            return fail(c, PGPU_ERR_OUT_OF_MEMORY, "pinned staging of %zu bytes", total + wide_cap);
         }
-        c->stage_cap = total;
+        c->stage_cap = total + wide_cap;
     }
     unsigned char* host = c->h_stage;
     // every byte is written below except geo_b of one-word primitives and the
     // alignment gaps; those are zeroed so that uploads are deterministic
     {
-        const size_t ends[][2] = {{off_nodes + (size_t)n_int * 64, off_wide},
-                                  {off_wide + (size_t)n_wide * kWideNodeFloat4 * 16, off_ga},
+        const size_t ends[][2] = {{off_nodes + (size_t)n_int * 64, off_ga},
                                   {off_ga + (size_t)n_leaf * 16, off_gb},
                                   {off_gb, off_vt},
                                   {off_vt + n_verts * 16, off_lm},
                                   {off_lm + (size_t)n_leaf * 4, off_lp},
                                   {off_lp + (size_t)n_leaf * 4, off_mt},
-                                  {off_mt + mats.size() * sizeof(DevMaterial), off_lt},
+                                  {off_mt + (size_t)s->n_materials * sizeof(DevMaterial), off_lt},
                                   {off_lt + lights.size() * sizeof(DevLight), total}};
         for (const auto& g : ends)
             if (g[1] > g[0]) std::memset(host + g[0], 0, g[1] - g[0]);
@@ -616,11 +603,30 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     float4* h_vt = reinterpret_cast<float4*>(host + off_vt);
     int* h_lm = reinterpret_cast<int*>(host + off_lm);
     int* h_lp = reinterpret_cast<int*>(host + off_lp);
-    for (int k = 0; k < s->n_mesh_vertices; ++k)
-        h_vt[k] = make_float4(s->mesh_vertices[3 * k], s->mesh_vertices[3 * k + 1],
-                              s->mesh_vertices[3 * k + 2], 0.0f);
+    DevMaterial* h_mt = reinterpret_cast<DevMaterial*>(host + off_mt);
+    parallel_for(s->n_materials, [&](int b, int e) {
+        for (int k = b; k < e; ++k) {
+            const pgpu_material& m = s->materials[k];
+            DevMaterial d{};
+            std::memcpy(d.albedo, m.albedo, 12);
+            d.kind = m.kind;
+            std::memcpy(d.emission, m.emission, 12);
+            d.reflectivity = m.reflectivity;
+            d.ior = m.ior;
+            d.specular = m.specular;
+            d.shininess = m.shininess;
+            std::memcpy(d.specular_color, m.specular_color, 12);
+            h_mt[k] = d;
+        }
+    });
+    for (int m : quad_mats) h_mt[m].area_emitter = 1;
+    if (!lights.empty()) std::memcpy(host + off_lt, lights.data(), lights.size() * sizeof(DevLight));
+    parallel_for(s->n_mesh_vertices, [&](int b, int e) {
+        for (int k = b; k < e; ++k)
+            h_vt[k] = make_float4(s->mesh_vertices[3 * k], s->mesh_vertices[3 * k + 1],
+                                  s->mesh_vertices[3 * k + 2], 0.0f);
+    });
     size_t next_vert = (size_t)s->n_mesh_vertices;
-    if (n_wide) std::memcpy(host + off_wide, wide.data(), (size_t)n_wide * kWideNodeFloat4 * 16);
     // explicit triangles take vertices in DFS leaf order: sequential then
     auto convert = [&](int kb, int ke) {
     for (int k = kb; k < ke; ++k) {
@@ -677,26 +683,74 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     };
     if (n_explicit_tri > 0) convert(0, n_nodes);
     else parallel_for(n_nodes, convert);
-    std::memcpy(host + off_mt, mats.data(), mats.size() * sizeof(DevMaterial));
-    std::memcpy(host + off_lt, lights.data(), lights.size() * sizeof(DevLight));
 
     PGPU_CUDA(c, cudaSetDevice(c->device));
     auto ds = std::make_unique<DeviceScene>();
+    // frees what was allocated when the upload fails from here on (stream
+    // ordered: after the copies already queued)
+    auto release = [&] {
+        if (ds->arena) cudaFreeAsync(ds->arena, c->stream);
+        if (ds->arena_wide) cudaFreeAsync(ds->arena_wide, c->stream);
+        cudaStreamSynchronize(c->stream);
+    };
     cudaError_t e = arena_alloc(c, total, &ds->arena);
-    if (e != cudaSuccess)
+    if (e != cudaSuccess) {
+        ds->arena = nullptr;
         return fail(c, PGPU_ERR_OUT_OF_MEMORY, "scene arena of %zu bytes: %s", total,
                     cudaGetErrorString(e));
-    ds->bytes = total;
+    }
     e = cudaMemcpyAsync(ds->arena, host, total, cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
-        cudaFreeAsync(ds->arena, c->stream);
+        release();
         return cuda_fail(c, e, "scene upload");
     }
+
+    // 4-wide nodes for the wavefront's traversal, built while the main part
+    // is in flight
+    std::vector<int>& leaf_ref = c->ws_leaf_ref;
+    leaf_ref.resize(n_nodes);
+    parallel_for(n_nodes, [&](int b, int e2) {
+        for (int k = b; k < e2; ++k) leaf_ref[k] = nodes[k].left < 0 ? ref_of(k) : 0;
+    });
+    int wide_stack = 0;
+    float4* h_wide = reinterpret_cast<float4*>(host + total);
+    const int n_wide = collapse_wide(nodes, n_nodes, leaf_ref, kMaxDepth, h_wide, c->ws_collapse,
+                                     wide_stack);
+    if (wide_stack > kMaxDepth) {
+        release();
+        return fail(c, PGPU_ERR_UNSUPPORTED, "BVH needs %d stack entries, more than %d",
+                    wide_stack, kMaxDepth);
+    }
+    const size_t wide_bytes = (size_t)n_wide * kWideNodeFloat4 * 16;
+    if (n_wide) {
+        e = arena_alloc(c, wide_bytes, &ds->arena_wide);
+        if (e != cudaSuccess) {
+            ds->arena_wide = nullptr;
+            release();
+            return fail(c, PGPU_ERR_OUT_OF_MEMORY, "wide-node arena of %zu bytes: %s", wide_bytes,
+                        cudaGetErrorString(e));
+        }
+        e = cudaMemcpyAsync(ds->arena_wide, h_wide, wide_bytes, cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) {
+            release();
+            return cuda_fail(c, e, "scene upload");
+        }
+    }
+    // host copy of the material table (material updates, glass flag) while
+    // the copies run; the last freed scene's vector has its pages mapped
+    std::vector<DevMaterial> mats = std::move(c->spare_mats);
+    c->spare_mats = {};
+    mats.assign(h_mt, h_mt + s->n_materials);
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(c, e, "scene upload");
+    }
+    ds->bytes = total + wide_bytes;
     unsigned char* base = static_cast<unsigned char*>(ds->arena);
     SceneView& v = ds->view;
     v.nodes = reinterpret_cast<const float4*>(base + off_nodes);
-    v.wide = n_wide ? reinterpret_cast<const float4*>(base + off_wide) : nullptr;
+    v.wide = n_wide ? static_cast<const float4*>(ds->arena_wide) : nullptr;
     v.geo_a = reinterpret_cast<const float4*>(base + off_ga);
     v.geo_b = reinterpret_cast<const float4*>(base + off_gb);
     v.verts = reinterpret_cast<const float4*>(base + off_vt);
@@ -741,6 +795,7 @@ int32_t pgpu_free_scene(pgpu_ctx* c, int32_t id) {
     // arena then returns to the pool
     cudaStreamSynchronize(c->stream);
     cudaFreeAsync(ds->arena, c->stream);
+    if (ds->arena_wide) cudaFreeAsync(ds->arena_wide, c->stream);
     if (ds->mats.capacity() > c->spare_mats.capacity()) c->spare_mats.swap(ds->mats);
     c->scenes.erase(id);
     return PGPU_OK;

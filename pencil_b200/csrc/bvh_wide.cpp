@@ -47,16 +47,16 @@ void write_node(float4* q, const float (&lo)[3][4], const float (&hi)[3][4], con
 
 // Copies each subtree's block into `out` at base[t], its interior refs
 // (local indices) shifted by base[t].
-void parallel_relocate(std::vector<float4>& out, const std::vector<std::vector<float4>>& local,
+void parallel_relocate(float4* out, const std::vector<std::vector<float4>>& local,
                        const std::vector<int>& count, const std::vector<int>& base) {
-    const int n = (int)local.size();
+    const int n = (int)count.size();
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
     const int T = std::max(1, std::min({16, hw, n}));
     std::atomic<int> next{0};
     auto worker = [&] {
         for (int t; (t = next.fetch_add(1)) < n;) {
             const int cnt = count[t];
-            float4* dst = out.data() + (size_t)base[t] * kWideNodeFloat4;
+            float4* dst = out + (size_t)base[t] * kWideNodeFloat4;
             std::copy_n(local[t].begin(), (size_t)cnt * kWideNodeFloat4, dst);
             for (int w = 0; w < cnt; ++w) {
                 int* refs = reinterpret_cast<int*>(dst + (size_t)w * kWideNodeFloat4 + 6);
@@ -134,7 +134,8 @@ struct Collapser {
 // kernels only follow refs), so the top comes first and each subtree's nodes
 // follow as one block in DFS pre-order.
 int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_ref,
-                      bool expand, int threads, std::vector<float4>& out, int& stack_need) {
+                      bool expand, int threads, float4* out, WideScratch& scratch,
+                      int& stack_need) {
     const int T = threads;
     // top: breadth-first over wide-node roots until enough subtrees wait
     struct Pending { int binary; int parent; int child; };   // ref slot to patch
@@ -188,11 +189,11 @@ int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_r
     }
     // remaining subtrees in parallel
     const int n_tasks = (int)(todo.size() - head);
-    std::vector<std::vector<float4>> local(n_tasks);
+    std::vector<std::vector<float4>>& local = scratch.local;
+    if ((int)local.size() < n_tasks) local.resize(n_tasks);
     std::vector<int> local_n(n_tasks, 0), local_need(n_tasks, 0);
     auto run = [&](int t) {
         Collapser c{nodes, leaf_ref, expand, local[t]};
-        local[t].reserve(1024);
         c.build(todo[head + t].binary, local_need[t]);
         local_n[t] = c.n_wide;
     };
@@ -209,8 +210,7 @@ int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_r
     std::vector<int> base(n_tasks);
     int total = n_top;
     for (int t = 0; t < n_tasks; ++t) { base[t] = total; total += local_n[t]; }
-    if (out.size() < (size_t)total * kWideNodeFloat4) out.resize((size_t)total * kWideNodeFloat4);
-    std::copy(top.begin(), top.end(), out.begin());
+    std::copy(top.begin(), top.end(), out);
     // which todo entry is which task: entries [head, end) are tasks; entries
     // before head became top nodes 0, 1, ... in order
     std::vector<int> wide_of_todo(todo.size());
@@ -218,7 +218,7 @@ int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_r
     for (int t = 0; t < n_tasks; ++t) wide_of_todo[head + t] = base[t];
     for (size_t k = 1; k < todo.size(); ++k) {
         const Pending& p = todo[k];
-        int* refs = reinterpret_cast<int*>(out.data() + (size_t)p.parent * kWideNodeFloat4 + 6);
+        int* refs = reinterpret_cast<int*>(out + (size_t)p.parent * kWideNodeFloat4 + 6);
         refs[p.child] = wide_of_todo[k];
     }
     parallel_relocate(out, local, local_n, base);
@@ -238,15 +238,11 @@ int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_r
 }  // namespace
 
 int collapse_wide(const pgpu_bvh_node* nodes, int n_nodes, const std::vector<int>& leaf_ref,
-                  int max_stack, std::vector<float4>& out, int& stack_need) {
+                  int max_stack, float4* out, WideScratch& scratch, int& stack_need) {
     stack_need = 0;
     if (n_nodes == 0 || nodes[0].left < 0) return 0;
-    int n_interior = 0;
-    for (int k = 0; k < n_nodes; ++k) n_interior += nodes[k].left >= 0;
-    // at most one wide node per binary interior node; `out` only grows, so a
-    // reused vector is neither reallocated nor cleared
-    if (out.size() < (size_t)n_interior * kWideNodeFloat4)
-        out.resize((size_t)n_interior * kWideNodeFloat4);
+    // a full binary tree of n_nodes nodes has (n_nodes - 1) / 2 interior ones
+    const int n_interior = (n_nodes - 1) / 2;
     // greedy collapse; if a pathological tree would need a deeper stack than
     // the kernels hold, two children per node (the binary tree's own bound)
     // threads only pay off for large trees
@@ -254,7 +250,7 @@ int collapse_wide(const pgpu_bvh_node* nodes, int n_nodes, const std::vector<int
     const int threads = n_interior < 16384 ? 1 : std::min(16, hw);
     int n_wide = 0;
     for (int pass = 0; pass < 2; ++pass) {
-        n_wide = collapse_parallel(nodes, leaf_ref, pass == 0, threads, out, stack_need);
+        n_wide = collapse_parallel(nodes, leaf_ref, pass == 0, threads, out, scratch, stack_need);
         if (stack_need <= max_stack) break;
     }
     return n_wide;

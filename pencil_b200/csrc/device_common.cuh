@@ -699,6 +699,25 @@ __device__ __forceinline__ unsigned leaf_bits(const int4& r) {
     return (r.x < 0 ? 1u : 0u) | (r.y < 0 ? 2u : 0u) | (r.z < 0 ? 4u : 0u) | (r.w < 0 ? 8u : 0u);
 }
 
+// Sorts four (key, ref) pairs by key, ascending (a five-exchange network).
+__device__ __forceinline__ void sort4(float& k0, int& r0, float& k1, int& r1, float& k2, int& r2,
+                                      float& k3, int& r3) {
+    auto cs = [](float& ka, int& ra, float& kb, int& rb) {
+        const bool sw = kb < ka;
+        const float tk = ka;
+        const int tr = ra;
+        ka = sw ? kb : ka;
+        ra = sw ? rb : ra;
+        kb = sw ? tk : kb;
+        rb = sw ? tr : rb;
+    };
+    cs(k0, r0, k1, r1);
+    cs(k2, r2, k3, r3);
+    cs(k0, r0, k2, r2);
+    cs(k1, r1, k3, r3);
+    cs(k1, r1, k2, r2);
+}
+
 // Resumable closest-hit traversal of the 4-wide tree. Same result rule as
 // ClosestTrav (smallest t, ties to the later DFS leaf); children are taken
 // nearest first, the others stacked with their entry distance.
@@ -760,20 +779,7 @@ struct ClosestTrav4 {
         float k2 = (m & 4u) && e[2] <= t_best ? e[2] : INFINITY;
         float k3 = (m & 8u) && e[3] <= t_best ? e[3] : INFINITY;
         int r0 = w.ref.x, r1 = w.ref.y, r2 = w.ref.z, r3 = w.ref.w;
-        auto cs = [](float& ka, int& ra, float& kb, int& rb) {
-            const bool sw = kb < ka;
-            const float tk = ka;
-            const int tr = ra;
-            ka = sw ? kb : ka;
-            ra = sw ? rb : ra;
-            kb = sw ? tk : kb;
-            rb = sw ? tr : rb;
-        };
-        cs(k0, r0, k1, r1);
-        cs(k2, r2, k3, r3);
-        cs(k0, r0, k2, r2);
-        cs(k1, r1, k3, r3);
-        cs(k1, r1, k2, r2);
+        sort4(k0, r0, k1, r1, k2, r2, k3, r3);
         if (k0 != INFINITY) {
             if (k3 != INFINITY) stk.push(sp++, r3, k3);
             if (k2 != INFINITY) stk.push(sp++, r2, k2);
@@ -794,7 +800,8 @@ struct ClosestTrav4 {
 
 // Resumable any-hit traversal of the 4-wide tree (BVHNode::occluded,
 // src/bvh.hpp:39-48): with a fixed t_max the set of boxes entered does not
-// depend on the order, so the answer equals the reference's.
+// depend on the order, so the answer equals the reference's whatever order
+// the children are taken in.
 template <int kShared, bool COUNT>
 struct AnyTrav4 {
     Ray ray;
@@ -844,14 +851,18 @@ struct AnyTrav4 {
             if (test_leaf(S, pick_ref(w.ref, k), cnt)) { hit = true; return true; }
         }
         if (m) {
-            const int k = __ffs(m) - 1;
-            m &= m - 1;
-            while (m) {
-                const int j = __ffs(m) - 1;
-                m &= m - 1;
-                stk.push(sp++, pick_ref(w.ref, j), 0.0f);
-            }
-            node = pick_ref(w.ref, k);
+            // nearest child first, the others stacked so that the nearer pop
+            // first: an occluder near the ray's origin ends the walk early
+            float k0 = (m & 1u) ? e[0] : INFINITY;
+            float k1 = (m & 2u) ? e[1] : INFINITY;
+            float k2 = (m & 4u) ? e[2] : INFINITY;
+            float k3 = (m & 8u) ? e[3] : INFINITY;
+            int r0 = w.ref.x, r1 = w.ref.y, r2 = w.ref.z, r3 = w.ref.w;
+            sort4(k0, r0, k1, r1, k2, r2, k3, r3);
+            if (k3 != INFINITY) stk.push(sp++, r3, 0.0f);
+            if (k2 != INFINITY) stk.push(sp++, r2, 0.0f);
+            if (k1 != INFINITY) stk.push(sp++, r1, 0.0f);
+            node = r0;
             return false;
         }
         if (sp == 0) return true;

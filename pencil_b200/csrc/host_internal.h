@@ -17,14 +17,21 @@ void build_bvh(const std::vector<pgpu_prim>& prims, std::vector<pgpu_bvh_node>& 
 int make_prim(int type, int material, const float* a, const float* b, const float* c, float s0,
               float s1, pgpu_prim* out);
 
+// Scratch memory of collapse_wide, kept by the caller between calls so that
+// repeated uploads reuse it instead of faulting in fresh pages.
+struct WideScratch {
+    std::vector<std::vector<float4>> local;   // one block per subtree task
+};
+
 // bvh_wide.cpp: 4-wide nodes (kWideNodeFloat4 float4 each) collapsed from a
-// validated binary tree in DFS pre-order, written to the front of `out`
-// (which grows as needed and is never shrunk). leaf_ref[k] is the leaf ref
-// of binary leaf k. Returns the number of wide nodes (0 when the root is a
-// leaf); stack_need receives the most stack entries a traversal holds, which
-// is at most max_stack unless the binary tree itself needs more.
+// validated binary tree in DFS pre-order, written to the front of `out`,
+// which must hold one wide node per binary interior node (there are never
+// more). leaf_ref[k] is the leaf ref of binary leaf k. Returns the number of
+// wide nodes (0 when the root is a leaf); stack_need receives the most stack
+// entries a traversal holds, which is at most max_stack unless the binary
+// tree itself needs more.
 int collapse_wide(const pgpu_bvh_node* nodes, int n_nodes, const std::vector<int>& leaf_ref,
-                  int max_stack, std::vector<float4>& out, int& stack_need);
+                  int max_stack, float4* out, WideScratch& scratch, int& stack_need);
 
 // Render configuration after validation.
 struct RenderCfg {
