@@ -97,7 +97,25 @@ struct WfArgs {
                               // unsorted one: it reads path state by slot)
     int* hist_e;
     int* chunk_off_e;
+    // A one-scene frame's scene and job, read from the kernel parameters
+    // (constant bank) by the ONE instantiations: a lane then finds its node
+    // and geometry pointers without a dependent global load per step.
+    SceneView view0;
+    WfJob job0;
 };
+
+// The scene / job of job index `jb`: the parameter copies in a one-scene
+// frame, the device tables otherwise.
+template <bool ONE>
+__device__ __forceinline__ const SceneView& view_of(const WfArgs& A, int jb) {
+    if constexpr (ONE) return A.view0;
+    else return A.views[A.jobs[jb].view];
+}
+template <bool ONE>
+__device__ __forceinline__ const WfJob& job_of(const WfArgs& A, int jb) {
+    if constexpr (ONE) return A.job0;
+    else return A.jobs[jb];
+}
 
 // Sort key of a ray: Morton code of its origin in the scene's root box
 // (kMortonBits per axis), then the octant of its direction.
@@ -208,7 +226,7 @@ __device__ __forceinline__ int fetch32(unsigned int* cursor) {
 }
 
 // ---- generate -----------------------------------------------------------------
-template <bool COUNT>
+template <bool COUNT, bool ONE>
 __global__ void __launch_bounds__(kWfBlock)
 wf_generate(WfArgs A, long long path_begin, int n_slots) {
     RayCount rc = {};
@@ -217,10 +235,10 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
     bool live = false;
     if (slot < n_slots) {
         long long path = path_begin + slot;
-        int jb = find_job(A.jobs, A.n_jobs, path);
-        const WfJob& J = A.jobs[jb];
+        const int jb = ONE ? 0 : find_job(A.jobs, A.n_jobs, path);
+        const WfJob& J = job_of<ONE>(A, jb);
         const PathParams& P = J.P;
-        const SceneView& S = A.views[J.view];
+        const SceneView& S = view_of<ONE>(A, jb);
         long long local = path - J.path_off;
         int pix = (int)(local / P.spp);
         int s = (int)(local % P.spp);
@@ -254,7 +272,7 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
 // between node steps; when few lanes of the warp are still busy, the idle
 // lanes take new rays from the queue (one atomic per warp), so warps keep
 // traversing instead of waiting for their slowest ray.
-template <bool COUNT>
+template <bool COUNT, bool ONE>
 __global__ void __launch_bounds__(kWfBlock)
 wf_extend(WfArgs A, int it) {
     extern __shared__ int smem[];
@@ -269,7 +287,11 @@ wf_extend(WfArgs A, int it) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     ClosestTrav4<kWfShared, COUNT> tr;
-    const SceneView* S = nullptr;
+    const SceneView* S = nullptr;       // the lane's scene (unused when ONE)
+    auto scene = [&]() -> const SceneView& {
+        if constexpr (ONE) return A.view0;
+        else return *S;
+    };
     int slot = -1;
     bool active = false;
     bool exhausted = false;
@@ -285,10 +307,11 @@ wf_extend(WfArgs A, int it) {
                 const int e = base + __popc(idle & below);
                 if (e < qv.total) {
                     slot = sorted_e ? A.qe[e] : qv.slot(e);
-                    S = &A.views[A.jobs[A.st[slot].w].view];
+                    if constexpr (!ONE) S = &A.views[A.jobs[A.st[slot].w].view];
                     const float4 o = A.ray_o[slot], d = A.ray_d[slot];
                     if (COUNT) rc.ext++;
-                    if (tr.init(*S, Ray{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)}, 1e-4f, 1e9f, &rc.tc))
+                    if (tr.init(scene(), Ray{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)}, 1e-4f, 1e9f,
+                                &rc.tc))
                         A.hit[slot] = make_float4(tr.t_best, __int_as_float(tr.best_ref),
                                                   __int_as_float(tr.best), 0.0f);
                     else
@@ -301,7 +324,7 @@ wf_extend(WfArgs A, int it) {
             if (exhausted) break;
             continue;
         }
-        if (active && tr.step(*S, stk, &rc.tc)) {
+        if (active && tr.step(scene(), stk, &rc.tc)) {
             A.hit[slot] = make_float4(tr.t_best, __int_as_float(tr.best_ref),
                                       __int_as_float(tr.best), 0.0f);
             active = false;
@@ -341,7 +364,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_extend_packet(WfArgs A) {
     RayCount rc = {};
     const QView qv = qview(A, 0);
     unsigned int* cursor = A.work + 0;
-    const SceneView& S = A.views[A.jobs[0].view];
+    const SceneView& S = A.view0;        // packets run in one-scene frames only
     while (true) {
         const int base = fetch32(cursor);
         if (base >= qv.total) break;
@@ -459,7 +482,7 @@ struct StoreNee {
     }
 };
 
-template <bool COUNT>
+template <bool COUNT, bool ONE>
 __global__ void __launch_bounds__(kWfBlock)
 wf_shade(WfArgs A, int it) {
     RayCount rc = {};
@@ -481,8 +504,8 @@ wf_shade(WfArgs A, int it) {
         if (e < qv.total) {
             slot = qv.slot(e);
             uint4 stv = A.st[slot];
-            const WfJob& J = A.jobs[stv.w];
-            const SceneView& S = A.views[J.view];
+            const WfJob& J = job_of<ONE>(A, stv.w);
+            const SceneView& S = view_of<ONE>(A, stv.w);
             float4 o = A.ray_o[slot], d = A.ray_d[slot], T = A.T[slot], L = A.L[slot];
             float4 hv = A.hit[slot];
             PathState ps;
@@ -641,7 +664,7 @@ wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
 // lane refill as extend. A lane owns one slot: it resolves the slot's records
 // in the order shade made them, feeding each visibility into the same
 // NeeAccum as the megakernel, then applies the pending terms to L.
-template <bool COUNT>
+template <bool COUNT, bool ONE>
 __global__ void __launch_bounds__(kWfBlock)
 wf_shadow(WfArgs A, int it) {
     extern __shared__ int smem[];
@@ -658,7 +681,11 @@ wf_shadow(WfArgs A, int it) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     AnyTrav4<kWfShared, COUNT> tr;
-    const SceneView* S = nullptr;
+    const SceneView* S = nullptr;       // the lane's scene (unused when ONE)
+    auto scene = [&]() -> const SceneView& {
+        if constexpr (ONE) return A.view0;
+        else return *S;
+    };
     NeeAccum acc;
     V3 L = v3(0, 0, 0), c = v3(0, 0, 0);
     int slot = -1, k = 0, n = 0, group_end = 0;
@@ -677,7 +704,7 @@ wf_shadow(WfArgs A, int it) {
             if (bits & 1) {
                 const float4 so = A.sh_o[idx], sd = A.sh_d[idx];
                 if (COUNT) rc.shadow++;
-                if (!tr.init(*S, Ray{v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z)}, so.w, sd.w,
+                if (!tr.init(scene(), Ray{v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z)}, so.w, sd.w,
                              &rc.tc))
                     return true;
                 acc.add(L, c, group_end, !tr.hit);
@@ -714,7 +741,7 @@ wf_shadow(WfArgs A, int it) {
                     const int info = __float_as_int(A.pt[slot].w);
                     const int kind = info & 3;
                     if (kind != 0) {
-                        S = &A.views[A.jobs[A.st[slot].w].view];
+                        if constexpr (!ONE) S = &A.views[A.jobs[A.st[slot].w].view];
                         const float4 L4 = A.L[slot];
                         if (kind == 1) {
                             acc.begin_pt();
@@ -735,7 +762,7 @@ wf_shadow(WfArgs A, int it) {
             if (exhausted) break;
             continue;
         }
-        if (active && tr.step(*S, stk, &rc.tc)) {
+        if (active && tr.step(scene(), stk, &rc.tc)) {
             acc.add(L, c, group_end, !tr.hit);
             ++k;
             active = advance();
@@ -814,6 +841,8 @@ struct WfScratch {
     WfJob* d_jobs = nullptr;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_key = 0;
+    SceneView graph_view0{};          // the parameters a one-scene graph was captured with
+    WfJob graph_job0{};
 };
 
 static size_t al(size_t x) { return (x + 255) & ~size_t(255); }
@@ -908,16 +937,16 @@ struct WfOccupancy {
     int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_scatter = 0, grid_packet = 0;
 };
 
-template <bool COUNT>
+template <bool COUNT, bool ONE>
 static cudaError_t occupancy(WfOccupancy& o) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     size_t smem = (size_t)kWfShared * kWfBlock * 8;
     int b1 = 0, b2 = 0, b3 = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, wf_extend<COUNT>, kWfBlock, smem);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, wf_shade<COUNT>, kWfBlock, 0);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, wf_shadow<COUNT>, kWfBlock, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, wf_extend<COUNT, ONE>, kWfBlock, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, wf_shade<COUNT, ONE>, kWfBlock, 0);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, wf_shadow<COUNT, ONE>, kWfBlock, smem);
     o.grid_extend = sms * std::max(b1, 1);
     o.grid_shade = sms * std::max(b2, 1);
     o.grid_shadow = sms * std::max(b3, 1);
@@ -957,13 +986,14 @@ struct LaunchTimer {
     }
 };
 
-template <bool COUNT>
+// ONE: a one-scene frame (W.args.view0 / job0 hold its scene and job).
+template <bool COUNT, bool ONE>
 static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& jobs, int iters,
                                  int Qeff, cudaStream_t st, int* launches, LaunchTimer& lt) {
     WfOccupancy occ;
-    cudaError_t e = occupancy<COUNT>(occ);
+    cudaError_t e = occupancy<COUNT, ONE>(occ);
     if (e != cudaSuccess) return e;
-    const bool packet_first = jobs.size() == 1 && W.args.packets != 0;
+    const bool packet_first = ONE && W.args.packets != 0;
     const WfArgs& A = W.args;
     const size_t smem = (size_t)kWfShared * kWfBlock * 8;
     // walk the path space in chunks of whole pixels
@@ -995,7 +1025,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
             return e;
         int gblocks = (int)((slots + kWfBlock - 1) / kWfBlock);
         lt.mark(KC_GENERATE, st, true);
-        wf_generate<COUNT><<<gblocks, kWfBlock, 0, st>>>(A, path_begin, (int)slots);
+        wf_generate<COUNT, ONE><<<gblocks, kWfBlock, 0, st>>>(A, path_begin, (int)slots);
         lt.mark(KC_GENERATE, st, false);
         n_launch += 1;
         for (int it = 0; it < iters; ++it) {
@@ -1003,7 +1033,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
             if (it == 0 && packet_first)
                 wf_extend_packet<COUNT><<<occ.grid_packet, kWfBlock, 0, st>>>(A);
             else
-                wf_extend<COUNT><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
+                wf_extend<COUNT, ONE><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
             lt.mark(KC_EXTEND, st, false);
             lt.mark(KC_SHADE, st, true);
             if (A.sort_key >= 2) {
@@ -1014,7 +1044,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
             if (sort_next &&
                 (e = cudaMemsetAsync(A.hist_e, 0, (size_t)kSortBins * 4, st)) != cudaSuccess)
                 return e;
-            wf_shade<COUNT><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
+            wf_shade<COUNT, ONE><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
             if (A.sort_key >= 2) {
                 wf_sort_scan<<<kSortChunks, kSortChunk, 0, st>>>(A.hist_s, A.chunk_off);
                 wf_sort_chunks<<<1, kSortChunk, 0, st>>>(A.chunk_off);
@@ -1033,7 +1063,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
             }
             lt.mark(KC_SHADE, st, false);
             lt.mark(KC_SHADOW, st, true);
-            wf_shadow<COUNT><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
+            wf_shadow<COUNT, ONE><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
             lt.mark(KC_SHADOW, st, false);
             n_launch += 3;
         }
@@ -1099,6 +1129,11 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     W.args.packets = packets ? 1 : 0;
     W.args.refill_below = refill > 0 ? refill : kDefaultRefill;
     W.args.maxS = maxS;
+    const bool one = n == 1;
+    if (one) {
+        W.args.view0 = views[jobs[0].view];
+        W.args.job0 = jobs[0];
+    }
     if ((e = cudaMemcpyAsync(W.d_views, views.data(), views.size() * sizeof(SceneView),
                              cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return e;
@@ -1121,18 +1156,29 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
         mix((unsigned long long)J.P.spp); mix((unsigned long long)J.P.depth);
     }
     mix((unsigned long long)iters);
+    mix((unsigned long long)one);
+    // a one-scene graph also bakes the scene and job into its kernel
+    // parameters: it is reused only while they are byte for byte the same
+    const bool same_params =
+        !one || (std::memcmp(&W.graph_view0, &W.args.view0, sizeof(SceneView)) == 0 &&
+                 std::memcmp(&W.graph_job0, &W.args.job0, sizeof(WfJob)) == 0);
     int nl = 0;
     LaunchTimer lt;
     lt.on = kernel_ms != nullptr;
+    auto enqueue = [&](int* nl_out) {
+        return count ? (one ? enqueue_frame<true, true>(W, jobs, iters, (int)Q, st, nl_out, lt)
+                            : enqueue_frame<true, false>(W, jobs, iters, (int)Q, st, nl_out, lt))
+                     : (one ? enqueue_frame<false, true>(W, jobs, iters, (int)Q, st, nl_out, lt)
+                            : enqueue_frame<false, false>(W, jobs, iters, (int)Q, st, nl_out, lt));
+    };
     if (lt.on) use_graph = false;
     if (use_graph) {
-        if (!W.graph || W.graph_key != key) {
+        if (!W.graph || W.graph_key != key || !same_params) {
             if (W.graph) { cudaGraphExecDestroy(W.graph); W.graph = nullptr; }
             cudaGraph_t g = nullptr;
             if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
                 return e;
-            cudaError_t ee = count ? enqueue_frame<true>(W, jobs, iters, (int)Q, st, &nl, lt)
-                                   : enqueue_frame<false>(W, jobs, iters, (int)Q, st, &nl, lt);
+            cudaError_t ee = enqueue(&nl);
             e = cudaStreamEndCapture(st, &g);
             if (ee != cudaSuccess) { if (g) cudaGraphDestroy(g); return ee; }
             if (e != cudaSuccess) return e;
@@ -1140,12 +1186,13 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
             cudaGraphDestroy(g);
             if (e != cudaSuccess) { W.graph = nullptr; return e; }
             W.graph_key = key;
+            W.graph_view0 = W.args.view0;
+            W.graph_job0 = W.args.job0;
         }
         if ((e = cudaGraphLaunch(W.graph, st)) != cudaSuccess) return e;
         if (launches) *launches = 1;
     } else {
-        e = count ? enqueue_frame<true>(W, jobs, iters, (int)Q, st, &nl, lt)
-                  : enqueue_frame<false>(W, jobs, iters, (int)Q, st, &nl, lt);
+        e = enqueue(&nl);
         if (e != cudaSuccess) return e;
         if (launches) *launches = nl;
         if (lt.on) {
@@ -1287,7 +1334,7 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
     A.counters = nullptr;
     A.sort_key = 0;
     A.refill_below = kDefaultRefill;
-    WfJob J;
+    WfJob J{};
     J.P = PathParams{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias,
                      c.salt, c.sample_offset, c.mis ? 1 : 0};
     J.view = 0;
@@ -1304,8 +1351,10 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
     if ((e = cudaMemcpyAsync(d_job, &J, sizeof(WfJob), cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return e;
     if ((e = cudaMemsetAsync(A.status, 0, 4, st)) != cudaSuccess) return e;
+    A.view0 = view;
+    A.job0 = J;
     WfOccupancy occ;
-    if ((e = occupancy<false>(occ)) != cudaSuccess) return e;
+    if ((e = occupancy<false, true>(occ)) != cudaSuccess) return e;
     const size_t smem = (size_t)kWfShared * kWfBlock * 8;
     const long long npix = (long long)c.W * c.H;
     const long long ppc = Q / c.spp;
@@ -1319,12 +1368,12 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
             return e;
         if ((e = cudaMemsetAsync(A.work, 0, (size_t)(c.depth + 2) * 3 * 4, st)) != cudaSuccess)
             return e;
-        wf_generate<false><<<(unsigned)((slots + kWfBlock - 1) / kWfBlock), kWfBlock, 0, st>>>(
+        wf_generate<false, true><<<(unsigned)((slots + kWfBlock - 1) / kWfBlock), kWfBlock, 0, st>>>(
             A, path0, (int)slots);
         for (int it = 0; it < c.depth; ++it) {
-            wf_extend<false><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
-            wf_shade<false><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
-            wf_shadow<false><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
+            wf_extend<false, true><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
+            wf_shade<false, true><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
+            wf_shadow<false, true><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
         }
         wf_accumulate<<<(unsigned)((pixels + kWfBlock - 1) / kWfBlock), kWfBlock, 0, st>>>(
             A, pix0, (int)pixels, path0);

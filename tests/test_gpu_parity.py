@@ -314,6 +314,29 @@ def test_batch_equals_individual_renders(gpu):
         gpu.free(s)
 
 
+def test_frame_graph_follows_the_scene(gpu):
+    """A one-scene wavefront frame runs as a CUDA graph whose kernel
+    parameters carry the scene; a second scene with the same frame shape
+    must not reuse the first scene's graph."""
+    from pencil_b200.renderer import GpuContext
+    jobs = W.sphere_batch(n_scenes=2, seed=23)
+    st = dataclasses.replace(jobs[0].settings, width=80, height=64, engine=A.ENGINE_WAVEFRONT)
+    sa, sb = (gpu.upload(j.scene) for j in jobs)
+    a1 = gpu.render(sa, st)
+    b = gpu.render(sb, st)
+    a2 = gpu.render(sa, st)
+    fresh = GpuContext(0)
+    try:
+        b_ref = fresh.render(fresh.upload(jobs[1].scene), st)
+    finally:
+        fresh.close()
+    assert np.array_equal(a1.view(np.uint32), a2.view(np.uint32))
+    assert np.array_equal(b.view(np.uint32), b_ref.view(np.uint32))
+    assert not np.array_equal(a1, b)
+    gpu.free(sa)
+    gpu.free(sb)
+
+
 def test_renders_are_deterministic(gpu, scenes):
     scene, fx, sid = scenes["prims_mix"]
     for eng in (A.ENGINE_MEGAKERNEL, A.ENGINE_WAVEFRONT):
