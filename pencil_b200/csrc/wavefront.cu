@@ -843,6 +843,11 @@ struct WfScratch {
     unsigned long long graph_key = 0;
     SceneView graph_view0{};          // the parameters a one-scene graph was captured with
     WfJob graph_job0{};
+    // second stream of a frame: bounce k's shadow kernel runs beside bounce
+    // k+1's extend kernel (created on first use, on the context's device)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_shaded = nullptr;  // shade k and its sorts are done
+    cudaEvent_t ev_shadow = nullptr;  // shadow k is done
 };
 
 static size_t al(size_t x) { return (x + 255) & ~size_t(255); }
@@ -994,6 +999,8 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
     cudaError_t e = occupancy<COUNT, ONE>(occ);
     if (e != cudaSuccess) return e;
     const bool packet_first = ONE && W.args.packets != 0;
+    // timed (profiled) frames stay on one stream so that kernel classes add up
+    const bool overlap = W.side != nullptr && !lt.on;
     const WfArgs& A = W.args;
     const size_t smem = (size_t)kWfShared * kWfBlock * 8;
     // walk the path space in chunks of whole pixels
@@ -1028,13 +1035,22 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         wf_generate<COUNT, ONE><<<gblocks, kWfBlock, 0, st>>>(A, path_begin, (int)slots);
         lt.mark(KC_GENERATE, st, false);
         n_launch += 1;
-        for (int it = 0; it < iters; ++it) {
+        // With a side stream, shadow k runs on it beside extend k+1 (they
+        // touch disjoint state: shadow k reads the shadow records and pending
+        // terms and adds to L, extend k+1 reads rays and writes hits); shade
+        // k+1 waits for both. Each kernel's tail then overlaps the other's.
+        auto launch_extend = [&](int it) {
             lt.mark(KC_EXTEND, st, true);
             if (it == 0 && packet_first)
                 wf_extend_packet<COUNT><<<occ.grid_packet, kWfBlock, 0, st>>>(A);
             else
                 wf_extend<COUNT, ONE><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
             lt.mark(KC_EXTEND, st, false);
+        };
+        if (iters > 0) launch_extend(0);
+        for (int it = 0; it < iters; ++it) {
+            if (overlap && it > 0 && (e = cudaStreamWaitEvent(st, W.ev_shadow, 0)) != cudaSuccess)
+                return e;
             lt.mark(KC_SHADE, st, true);
             if (A.sort_key >= 2) {
                 if ((e = cudaMemsetAsync(A.hist_s, 0, (size_t)kSortBins * 4, st)) != cudaSuccess)
@@ -1062,11 +1078,22 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
                 n_launch += 3;
             }
             lt.mark(KC_SHADE, st, false);
-            lt.mark(KC_SHADOW, st, true);
-            wf_shadow<COUNT, ONE><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
-            lt.mark(KC_SHADOW, st, false);
+            if (overlap) {
+                if ((e = cudaEventRecord(W.ev_shaded, st)) != cudaSuccess) return e;
+                if ((e = cudaStreamWaitEvent(W.side, W.ev_shaded, 0)) != cudaSuccess) return e;
+                wf_shadow<COUNT, ONE><<<occ.grid_shadow, kWfBlock, smem, W.side>>>(A, it);
+                if ((e = cudaEventRecord(W.ev_shadow, W.side)) != cudaSuccess) return e;
+                if (it + 1 < iters) launch_extend(it + 1);
+            } else {
+                lt.mark(KC_SHADOW, st, true);
+                wf_shadow<COUNT, ONE><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
+                lt.mark(KC_SHADOW, st, false);
+                if (it + 1 < iters) launch_extend(it + 1);
+            }
             n_launch += 3;
         }
+        if (overlap && iters > 0 && (e = cudaStreamWaitEvent(st, W.ev_shadow, 0)) != cudaSuccess)
+            return e;
         int ablocks = (int)((pixels + kWfBlock - 1) / kWfBlock);
         lt.mark(KC_ACCUMULATE, st, true);
         wf_accumulate<<<ablocks, kWfBlock, 0, st>>>(A, pix_begin, (int)pixels, path_begin);
@@ -1141,6 +1168,12 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
                              cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return e;
     if ((e = cudaMemsetAsync(W.args.status, 0, 4, st)) != cudaSuccess) return e;
+    if (!W.side) {
+        if ((e = cudaStreamCreateWithFlags(&W.side, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&W.ev_shaded, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&W.ev_shadow, cudaEventDisableTiming)) != cudaSuccess)
+            return e;
+    }
     // A graph is reused while the frame's shape is unchanged.
     unsigned long long key = 1469598103934665603ull;
     auto mix = [&](unsigned long long v) { key = (key ^ v) * 1099511628211ull; };
@@ -1179,8 +1212,21 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
             if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
                 return e;
             cudaError_t ee = enqueue(&nl);
+            if (ee != cudaSuccess) {
+                // a failed enqueue may leave the side stream forked off the
+                // capture: join it so that the capture ends on both streams
+                cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+                if (cudaStreamIsCapturing(W.side, &cs) == cudaSuccess &&
+                    cs != cudaStreamCaptureStatusNone &&
+                    cudaEventRecord(W.ev_shadow, W.side) == cudaSuccess)
+                    cudaStreamWaitEvent(st, W.ev_shadow, 0);
+            }
             e = cudaStreamEndCapture(st, &g);
-            if (ee != cudaSuccess) { if (g) cudaGraphDestroy(g); return ee; }
+            if (ee != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                (void)cudaGetLastError();   // the failure is reported once, here
+                return ee;
+            }
             if (e != cudaSuccess) return e;
             e = cudaGraphInstantiate(&W.graph, g, 0);
             cudaGraphDestroy(g);
@@ -1221,6 +1267,9 @@ WfScratch* wavefront_new() { return new WfScratch(); }
 void wavefront_delete(WfScratch* W) {
     if (!W) return;
     wavefront_release(*W);
+    if (W->ev_shaded) cudaEventDestroy(W->ev_shaded);
+    if (W->ev_shadow) cudaEventDestroy(W->ev_shadow);
+    if (W->side) cudaStreamDestroy(W->side);
     delete W;
 }
 
