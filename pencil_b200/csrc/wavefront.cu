@@ -44,6 +44,11 @@ constexpr int kDefaultRefill = 20;   // lanes still busy when a warp refetches
 // traverse alike (2^21 bins; a counting sort per iteration).
 constexpr int kMortonBits = 6;
 constexpr int kSortBins = 1 << (3 * kMortonBits + 3);
+// Sort key 3 also orders each iteration's extension rays, by the same kind of
+// key at kMortonBitsE bits per axis (2^18 bins: coarser cells sort the
+// extension rays as well for a cheaper histogram and scan).
+constexpr int kMortonBitsE = 5;
+constexpr int kSortBinsE = 1 << (3 * kMortonBitsE + 3);
 
 // One render job of the path space.
 struct WfJob {
@@ -127,8 +132,9 @@ __device__ __forceinline__ uint32_t spread_bits3(uint32_t x) {
     x = (x | (x << 2)) & 0x09249249u;
     return x;
 }
+template <int BITS = kMortonBits>
 __device__ __forceinline__ int sort_key_of(const SceneView& S, V3 o, V3 d) {
-    const float cells = (float)(1 << kMortonBits);
+    const float cells = (float)(1 << BITS);
     uint32_t c[3];
     const float oo[3] = {o.x, o.y, o.z};
 #pragma unroll
@@ -136,7 +142,7 @@ __device__ __forceinline__ int sort_key_of(const SceneView& S, V3 o, V3 d) {
         const float ext = S.root_max[a] - S.root_min[a];
         const float f = ext > 0.0f ? (oo[a] - S.root_min[a]) * (cells / ext) : 0.0f;
         const int q = f > 0.0f ? (int)f : 0;   // NaN and below the box: cell 0
-        c[a] = (uint32_t)min(q, (1 << kMortonBits) - 1);
+        c[a] = (uint32_t)min(q, (1 << BITS) - 1);
     }
     const uint32_t m = spread_bits3(c[0]) | (spread_bits3(c[1]) << 1) | (spread_bits3(c[2]) << 2);
     const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
@@ -257,12 +263,19 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
         if (COUNT) rc.ref++;
         live = P.depth > 0;
     }
-    unsigned m = __ballot_sync(0xffffffffu, live);
-    if (m) {
-        int first = 0;
-        if (lane == __ffs(m) - 1) first = atomicAdd(A.counts, __popc(m));
-        first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
-        if (live) A.q[0][first + __popc(m & ((1u << lane) - 1u))] = slot;
+    if constexpr (ONE) {
+        // one job: either every path of the chunk is live or none is, so the
+        // first queue is the slot order itself (no append atomics)
+        if (live) A.q[0][slot] = slot;
+        if (slot == 0 && A.job0.P.depth > 0) A.counts[0] = n_slots;
+    } else {
+        unsigned m = __ballot_sync(0xffffffffu, live);
+        if (m) {
+            int first = 0;
+            if (lane == __ffs(m) - 1) first = atomicAdd(A.counts, __popc(m));
+            first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
+            if (live) A.q[0][first + __popc(m & ((1u << lane) - 1u))] = slot;
+        }
     }
     flush_counts<COUNT>(A, rc);
 }
@@ -482,8 +495,10 @@ struct StoreNee {
     }
 };
 
+// At most 80 registers (6 blocks per SM): the shading state machine is
+// latency-bound, and the extra resident warps pay for a few spilled words.
 template <bool COUNT, bool ONE>
-__global__ void __launch_bounds__(kWfBlock)
+__global__ void __launch_bounds__(kWfBlock, 6)
 wf_shade(WfArgs A, int it) {
     RayCount rc = {};
     QView qv = qview(A, it);
@@ -538,7 +553,7 @@ wf_shade(WfArgs A, int it) {
                     bin = (ps.ray.d.x < 0.0f ? 1 : 0) | (ps.ray.d.y < 0.0f ? 2 : 0) |
                           (ps.ray.d.z < 0.0f ? 4 : 0);
                 if (A.sort_key == 3) {
-                    key_next = sort_key_of(S, ps.ray.o, ps.ray.d);
+                    key_next = sort_key_of<kMortonBitsE>(S, ps.ray.o, ps.ray.d);
                     A.key_e[slot] = key_next;
                 }
             }
@@ -577,6 +592,9 @@ wf_shade(WfArgs A, int it) {
 // chunk_off[key / kSortChunk] plus its bin's running local offset.
 constexpr int kSortChunk = 1024;
 constexpr int kSortChunks = kSortBins / kSortChunk;
+constexpr int kSortChunksE = kSortBinsE / kSortChunk;
+static_assert(kSortBins % kSortChunk == 0 && kSortBinsE % kSortChunk == 0,
+              "the bin scan works on whole chunks");
 
 // Exclusive scan of one value per thread of a 1024-thread block; returns the
 // block total through *total.
@@ -613,15 +631,16 @@ __global__ void __launch_bounds__(kSortChunk) wf_sort_scan(int* hist, int* chunk
     if (threadIdx.x == 0) chunk_off[blockIdx.x] = total;
 }
 
+template <int CHUNKS>
 __global__ void __launch_bounds__(kSortChunk) wf_sort_chunks(int* chunk_off) {
     __shared__ int s_warp[32];
-    constexpr int per = (kSortChunks + kSortChunk - 1) / kSortChunk;
+    constexpr int per = (CHUNKS + kSortChunk - 1) / kSortChunk;
     int v[per];
     int sum = 0;
 #pragma unroll
     for (int k = 0; k < per; ++k) {
         const int c = threadIdx.x * per + k;
-        v[k] = c < kSortChunks ? chunk_off[c] : 0;
+        v[k] = c < CHUNKS ? chunk_off[c] : 0;
         sum += v[k];
     }
     int total = 0;
@@ -629,7 +648,7 @@ __global__ void __launch_bounds__(kSortChunk) wf_sort_chunks(int* chunk_off) {
 #pragma unroll
     for (int k = 0; k < per; ++k) {
         const int c = threadIdx.x * per + k;
-        if (c < kSortChunks) chunk_off[c] = run;
+        if (c < CHUNKS) chunk_off[c] = run;
         run += v[k];
     }
 }
@@ -772,45 +791,59 @@ wf_shadow(WfArgs A, int it) {
 }
 
 // ---- accumulate -----------------------------------------------------------------
-// One thread per pixel of the chunk: sums in the megakernel's lane order
-// (lane g takes samples g, g+G, ...; lanes combined by a butterfly).
+// One warp per pixel of the chunk: lane g < G (the job's accumulation lanes)
+// sums samples g, g+G, ... in order and the lanes are combined by the
+// megakernel's halving tree, so the sums round exactly as the megakernel's;
+// a warp's loads of a pixel's samples are contiguous.
 __global__ void __launch_bounds__(kWfBlock)
 wf_accumulate(WfArgs A, long long pix_begin, int n_pix, long long path_begin) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n_pix) return;
-    long long pix = pix_begin + k;
-    int jb = find_job_pix(A.jobs, A.n_jobs, pix);
+    const long long k = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int g = threadIdx.x & 31;
+    if (k >= n_pix) return;                  // whole warps
+    const long long pix = pix_begin + k;
+    const int jb = find_job_pix(A.jobs, A.n_jobs, pix);
     const WfJob& J = A.jobs[jb];
-    int spp = J.P.spp, G = J.G;
-    long long lp = pix - J.pix_off;
-    long long first = J.path_off + lp * spp - path_begin;
-    V3 acc[32], acc2[32];
-    for (int g = 0; g < G; ++g) { acc[g] = v3(0, 0, 0); acc2[g] = v3(0, 0, 0); }
-    for (int g = 0; g < G; ++g) {
+    const int spp = J.P.spp, G = J.G;
+    const long long lp = pix - J.pix_off;
+    const long long first = J.path_off + lp * spp - path_begin;
+    V3 acc = v3(0, 0, 0), acc2 = v3(0, 0, 0);
+    if (g < G) {
         for (int s = g; s < spp; s += G) {
-            float4 l = A.L[first + s];
-            V3 c = v3(l.x, l.y, l.z);
-            acc[g] = acc[g] + c;
-            acc2[g] = acc2[g] + c * c;
+            const float4 l = A.L[first + s];
+            const V3 c = v3(l.x, l.y, l.z);
+            acc = acc + c;
+            acc2 = acc2 + c * c;
         }
     }
     for (int off = G >> 1; off > 0; off >>= 1) {
-        for (int g = 0; g < off; ++g) {
-            acc[g] = acc[g] + acc[g + off];
-            acc2[g] = acc2[g] + acc2[g + off];
+        const V3 o = v3(__shfl_down_sync(0xffffffffu, acc.x, off),
+                        __shfl_down_sync(0xffffffffu, acc.y, off),
+                        __shfl_down_sync(0xffffffffu, acc.z, off));
+        const V3 o2 = v3(__shfl_down_sync(0xffffffffu, acc2.x, off),
+                         __shfl_down_sync(0xffffffffu, acc2.y, off),
+                         __shfl_down_sync(0xffffffffu, acc2.z, off));
+        if (g < off) {
+            acc = acc + o;
+            acc2 = acc2 + o2;
         }
     }
+    if (g != 0) return;
     const float denom = (float)spp;
     float* o = J.out + 3 * lp;
-    o[0] = acc[0].x / denom;
-    o[1] = acc[0].y / denom;
-    o[2] = acc[0].z / denom;
+    o[0] = acc.x / denom;
+    o[1] = acc.y / denom;
+    o[2] = acc.z / denom;
     if (J.m2) {
         float* q = J.m2 + 3 * lp;
-        q[0] = acc2[0].x / denom;
-        q[1] = acc2[0].y / denom;
-        q[2] = acc2[0].z / denom;
+        q[0] = acc2.x / denom;
+        q[1] = acc2.y / denom;
+        q[2] = acc2.z / denom;
     }
+}
+
+// Blocks of wf_accumulate for `pixels` pixels (a warp each).
+static unsigned accumulate_blocks(long long pixels) {
+    return (unsigned)((pixels * 32 + kWfBlock - 1) / kWfBlock);
 }
 
 // ---- host side ------------------------------------------------------------------
@@ -874,8 +907,8 @@ static cudaError_t ensure_scratch(WfScratch& W, int Q, int maxS, int iters, int 
     sz += al((size_t)(iters + 2) * 3 * 4);           // work cursors
     sz += al(4);                                     // status
     sz += 5 * al((size_t)Q * 4);                     // sort: keys, list, sorted queues
-    sz += 2 * al((size_t)kSortBins * 4);             // sort: bin histograms
-    sz += 2 * al((size_t)kSortChunks * 4);           // sort: chunk offsets
+    sz += al((size_t)kSortBins * 4) + al((size_t)kSortBinsE * 4);        // sort: histograms
+    sz += al((size_t)kSortChunks * 4) + al((size_t)kSortChunksE * 4);    // chunk offsets
     sz += al((size_t)(iters + 2) * 2 * 4);           // sort: list counts
     sz += al((size_t)n_views * sizeof(SceneView));
     sz += al((size_t)n_jobs * sizeof(WfJob));
@@ -916,8 +949,8 @@ static cudaError_t ensure_scratch(WfScratch& W, int Q, int maxS, int iters, int 
     A.chunk_off = reinterpret_cast<int*>(take((size_t)kSortChunks * 4));
     A.key_e = reinterpret_cast<int*>(take((size_t)Q * 4));
     A.qe = reinterpret_cast<int*>(take((size_t)Q * 4));
-    A.hist_e = reinterpret_cast<int*>(take((size_t)kSortBins * 4));
-    A.chunk_off_e = reinterpret_cast<int*>(take((size_t)kSortChunks * 4));
+    A.hist_e = reinterpret_cast<int*>(take((size_t)kSortBinsE * 4));
+    A.chunk_off_e = reinterpret_cast<int*>(take((size_t)kSortChunksE * 4));
     A.tcnt = reinterpret_cast<int*>(take((size_t)(iters + 2) * 2 * 4));
     W.d_views = reinterpret_cast<SceneView*>(take((size_t)n_views * sizeof(SceneView)));
     W.d_jobs = reinterpret_cast<WfJob*>(take((size_t)n_jobs * sizeof(WfJob)));
@@ -1058,20 +1091,20 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
             }
             const bool sort_next = A.sort_key == 3 && it + 1 < iters;
             if (sort_next &&
-                (e = cudaMemsetAsync(A.hist_e, 0, (size_t)kSortBins * 4, st)) != cudaSuccess)
+                (e = cudaMemsetAsync(A.hist_e, 0, (size_t)kSortBinsE * 4, st)) != cudaSuccess)
                 return e;
             wf_shade<COUNT, ONE><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
             if (A.sort_key >= 2) {
                 wf_sort_scan<<<kSortChunks, kSortChunk, 0, st>>>(A.hist_s, A.chunk_off);
-                wf_sort_chunks<<<1, kSortChunk, 0, st>>>(A.chunk_off);
+                wf_sort_chunks<kSortChunks><<<1, kSortChunk, 0, st>>>(A.chunk_off);
                 wf_sort_scatter<<<occ.grid_scatter, kWfBlock, 0, st>>>(
                     A.tmp_s, A.tcnt + 2 * it + 1, A.key_s, A.hist_s, A.chunk_off, A.qs);
                 n_launch += 3;
             }
             if (sort_next) {
                 // the survivors shade just queued (unsorted) -> qe in key order
-                wf_sort_scan<<<kSortChunks, kSortChunk, 0, st>>>(A.hist_e, A.chunk_off_e);
-                wf_sort_chunks<<<1, kSortChunk, 0, st>>>(A.chunk_off_e);
+                wf_sort_scan<<<kSortChunksE, kSortChunk, 0, st>>>(A.hist_e, A.chunk_off_e);
+                wf_sort_chunks<kSortChunksE><<<1, kSortChunk, 0, st>>>(A.chunk_off_e);
                 wf_sort_scatter<<<occ.grid_scatter, kWfBlock, 0, st>>>(
                     A.q[(it + 1) & 1], A.counts + (it + 1) * kOctants, A.key_e, A.hist_e,
                     A.chunk_off_e, A.qe);
@@ -1094,7 +1127,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         }
         if (overlap && iters > 0 && (e = cudaStreamWaitEvent(st, W.ev_shadow, 0)) != cudaSuccess)
             return e;
-        int ablocks = (int)((pixels + kWfBlock - 1) / kWfBlock);
+        const unsigned ablocks = accumulate_blocks(pixels);
         lt.mark(KC_ACCUMULATE, st, true);
         wf_accumulate<<<ablocks, kWfBlock, 0, st>>>(A, pix_begin, (int)pixels, path_begin);
         lt.mark(KC_ACCUMULATE, st, false);
@@ -1424,7 +1457,7 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
             wf_shade<false, true><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
             wf_shadow<false, true><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
         }
-        wf_accumulate<<<(unsigned)((pixels + kWfBlock - 1) / kWfBlock), kWfBlock, 0, st>>>(
+        wf_accumulate<<<accumulate_blocks(pixels), kWfBlock, 0, st>>>(
             A, pix0, (int)pixels, path0);
         n_launch += 2 + 3 * c.depth;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
