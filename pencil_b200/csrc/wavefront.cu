@@ -791,16 +791,12 @@ wf_shadow(WfArgs A, int it) {
 }
 
 // ---- accumulate -----------------------------------------------------------------
-// One warp per pixel of the chunk: lane g < G (the job's accumulation lanes)
-// sums samples g, g+G, ... in order and the lanes are combined by the
+// The sums of one pixel by its warp: lane g < G (the job's accumulation
+// lanes) sums samples g, g+G, ... in order and the lanes are combined by the
 // megakernel's halving tree, so the sums round exactly as the megakernel's;
-// a warp's loads of a pixel's samples are contiguous.
-__global__ void __launch_bounds__(kWfBlock)
-wf_accumulate(WfArgs A, long long pix_begin, int n_pix, long long path_begin) {
-    const long long k = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const int g = threadIdx.x & 31;
-    if (k >= n_pix) return;                  // whole warps
-    const long long pix = pix_begin + k;
+// the warp's loads of the pixel's samples are contiguous.
+__device__ __forceinline__ void accumulate_pixel(const WfArgs& A, long long pix,
+                                                 long long path_begin, int g) {
     const int jb = find_job_pix(A.jobs, A.n_jobs, pix);
     const WfJob& J = A.jobs[jb];
     const int spp = J.P.spp, G = J.G;
@@ -841,9 +837,20 @@ wf_accumulate(WfArgs A, long long pix_begin, int n_pix, long long path_begin) {
     }
 }
 
-// Blocks of wf_accumulate for `pixels` pixels (a warp each).
-static unsigned accumulate_blocks(long long pixels) {
-    return (unsigned)((pixels * 32 + kWfBlock - 1) / kWfBlock);
+// A warp per pixel of the chunk, grid-stride over the pixels.
+__global__ void __launch_bounds__(kWfBlock)
+wf_accumulate(WfArgs A, long long pix_begin, int n_pix, long long path_begin) {
+    const int g = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long k = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; k < n_pix;
+         k += warps)
+        accumulate_pixel(A, pix_begin + k, path_begin, g);
+}
+
+// Blocks of wf_accumulate for `pixels` pixels: a warp each, at most `cap`.
+static unsigned accumulate_blocks(long long pixels, int cap) {
+    const long long b = (pixels * 32 + kWfBlock - 1) / kWfBlock;
+    return (unsigned)(b < cap ? b : cap);
 }
 
 // ---- host side ------------------------------------------------------------------
@@ -973,6 +980,7 @@ static int max_shadow_records(const SceneView& v, const std::vector<DevLight>& l
 
 struct WfOccupancy {
     int grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_scatter = 0, grid_packet = 0;
+    int grid_accumulate = 0;
 };
 
 template <bool COUNT, bool ONE>
@@ -989,6 +997,7 @@ static cudaError_t occupancy(WfOccupancy& o) {
     o.grid_shade = sms * std::max(b2, 1);
     o.grid_shadow = sms * std::max(b3, 1);
     o.grid_scatter = sms * 8;
+    o.grid_accumulate = sms * 16;
     int b4 = 0;
     if (e == cudaSuccess)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, wf_extend_packet<COUNT>, kWfBlock, 0);
@@ -1127,7 +1136,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         }
         if (overlap && iters > 0 && (e = cudaStreamWaitEvent(st, W.ev_shadow, 0)) != cudaSuccess)
             return e;
-        const unsigned ablocks = accumulate_blocks(pixels);
+        const unsigned ablocks = accumulate_blocks(pixels, occ.grid_accumulate);
         lt.mark(KC_ACCUMULATE, st, true);
         wf_accumulate<<<ablocks, kWfBlock, 0, st>>>(A, pix_begin, (int)pixels, path_begin);
         lt.mark(KC_ACCUMULATE, st, false);
@@ -1457,7 +1466,7 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
             wf_shade<false, true><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
             wf_shadow<false, true><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
         }
-        wf_accumulate<<<accumulate_blocks(pixels), kWfBlock, 0, st>>>(
+        wf_accumulate<<<accumulate_blocks(pixels, occ.grid_accumulate), kWfBlock, 0, st>>>(
             A, pix0, (int)pixels, path0);
         n_launch += 2 + 3 * c.depth;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
