@@ -123,6 +123,7 @@ __device__ __forceinline__ void sample_uv(int i, int j, int sx, int sy, int W, i
 struct RayPre {
     V3 o, inv;
     bool nx, ny, nz;  // inv < 0: near plane is the box max
+    int ox, oy, oz;   // 4-wide nodes: float4 offset of the near planes (0: lo, 3: hi)
 };
 __device__ __forceinline__ RayPre prep(const Ray& r) {
     RayPre p;
@@ -131,6 +132,9 @@ __device__ __forceinline__ RayPre prep(const Ray& r) {
     p.nx = p.inv.x < 0.0f;
     p.ny = p.inv.y < 0.0f;
     p.nz = p.inv.z < 0.0f;
+    p.ox = p.nx ? 3 : 0;
+    p.oy = p.ny ? 3 : 0;
+    p.oz = p.nz ? 3 : 0;
     return p;
 }
 
@@ -657,22 +661,42 @@ struct AnyTrav {
 };
 
 // ---- 4-wide traversal (wavefront) ------------------------------------------------
-// One wide node: its four child boxes (SoA float4 per plane) and refs.
+// One wide node as one ray sees it: its four child boxes' near and far
+// planes per axis (SoA float4 each) and refs. A node stores the lo planes of
+// x, y, z, then the hi planes; the ray's octant picks which are near, so the
+// loads, not per-child selects, put the planes in slab order.
 struct WideNode {
-    float4 lx, ly, lz, hx, hy, hz;
+    float4 nr[3], fr[3];
     int4 ref;
 };
-__device__ __forceinline__ WideNode load_wide(const float4* wide, int node) {
+__device__ __forceinline__ WideNode load_wide(const float4* wide, int node, const RayPre& r) {
     const float4* np = wide + (size_t)kWideNodeFloat4 * node;
     WideNode w;
-    w.lx = __ldg(np);
-    w.ly = __ldg(np + 1);
-    w.lz = __ldg(np + 2);
-    w.hx = __ldg(np + 3);
-    w.hy = __ldg(np + 4);
-    w.hz = __ldg(np + 5);
+    w.nr[0] = __ldg(np + r.ox);
+    w.fr[0] = __ldg(np + 3 - r.ox);
+    w.nr[1] = __ldg(np + 1 + r.oy);
+    w.fr[1] = __ldg(np + 4 - r.oy);
+    w.nr[2] = __ldg(np + 2 + r.oz);
+    w.fr[2] = __ldg(np + 5 - r.oz);
     w.ref = __ldg(reinterpret_cast<const int4*>(np + 6));
     return w;
+}
+
+// AABB::hit with the near and far planes already chosen (the same
+// arithmetic as slab).
+__device__ __forceinline__ bool slab_nf(float nx, float ny, float nz, float fx, float fy,
+                                        float fz, const RayPre& r, float tmin, float tmax,
+                                        float& entry) {
+    const float t0x = (nx - r.o.x) * r.inv.x;
+    const float t1x = (fx - r.o.x) * r.inv.x;
+    const float t0y = (ny - r.o.y) * r.inv.y;
+    const float t1y = (fy - r.o.y) * r.inv.y;
+    const float t0z = (nz - r.o.z) * r.inv.z;
+    const float t1z = (fz - r.o.z) * r.inv.z;
+    const float en = fmax3f(fmaxf(tmin, t0x), t0y, t0z);
+    const float ex = fmin3f(fminf(tmax, t1x), t1y, t1z);
+    entry = en;
+    return !(ex < en);
 }
 
 // Slab tests of the four children: bit k of the result is child k's hit,
@@ -680,10 +704,14 @@ __device__ __forceinline__ WideNode load_wide(const float4* wide, int node) {
 __device__ __forceinline__ unsigned slab4(const WideNode& w, const RayPre& r, float tmin,
                                           float tmax, float (&e)[4]) {
     unsigned m = 0;
-    m |= slab(w.lx.x, w.ly.x, w.lz.x, w.hx.x, w.hy.x, w.hz.x, r, tmin, tmax, e[0]) ? 1u : 0u;
-    m |= slab(w.lx.y, w.ly.y, w.lz.y, w.hx.y, w.hy.y, w.hz.y, r, tmin, tmax, e[1]) ? 2u : 0u;
-    m |= slab(w.lx.z, w.ly.z, w.lz.z, w.hx.z, w.hy.z, w.hz.z, r, tmin, tmax, e[2]) ? 4u : 0u;
-    m |= slab(w.lx.w, w.ly.w, w.lz.w, w.hx.w, w.hy.w, w.hz.w, r, tmin, tmax, e[3]) ? 8u : 0u;
+    m |= slab_nf(w.nr[0].x, w.nr[1].x, w.nr[2].x, w.fr[0].x, w.fr[1].x, w.fr[2].x, r, tmin,
+                 tmax, e[0]) ? 1u : 0u;
+    m |= slab_nf(w.nr[0].y, w.nr[1].y, w.nr[2].y, w.fr[0].y, w.fr[1].y, w.fr[2].y, r, tmin,
+                 tmax, e[1]) ? 2u : 0u;
+    m |= slab_nf(w.nr[0].z, w.nr[1].z, w.nr[2].z, w.fr[0].z, w.fr[1].z, w.fr[2].z, r, tmin,
+                 tmax, e[2]) ? 4u : 0u;
+    m |= slab_nf(w.nr[0].w, w.nr[1].w, w.nr[2].w, w.fr[0].w, w.fr[1].w, w.fr[2].w, r, tmin,
+                 tmax, e[3]) ? 8u : 0u;
     return m;
 }
 
@@ -762,7 +790,7 @@ struct ClosestTrav4 {
 
     __device__ __forceinline__ bool step(const SceneView& S, TravStack<kShared>& stk,
                                          TravCount* cnt) {
-        const WideNode w = load_wide(S.wide, node);
+        const WideNode w = load_wide(S.wide, node, rp);
         if (COUNT) cnt->nodes++;
         float e[4];
         unsigned m = slab4(w, rp, tmin, t_best, e);
@@ -839,7 +867,7 @@ struct AnyTrav4 {
 
     __device__ __forceinline__ bool step(const SceneView& S, TravStack<kShared>& stk,
                                          TravCount* cnt) {
-        const WideNode w = load_wide(S.wide, node);
+        const WideNode w = load_wide(S.wide, node, rp);
         if (COUNT) cnt->nodes++;
         float e[4];
         unsigned m = slab4(w, rp, tmin, tmax, e);

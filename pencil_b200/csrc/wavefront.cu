@@ -391,10 +391,13 @@ __global__ void __launch_bounds__(kWfBlock) wf_extend_packet(WfArgs A) {
             if (COUNT) rc.ext++;
             active = !tr.init(S, Ray{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)}, 1e-4f, 1e9f, &rc.tc);
         }
+        // lanes without a ray still load each node the packet enters: give
+        // them the lo-first plane order
+        if (!active) tr.rp.ox = tr.rp.oy = tr.rp.oz = 0;
         if (__any_sync(0xffffffffu, active)) {
             int node = 0, sp = 0;
             while (true) {
-                const WideNode w = load_wide(S.wide, node);
+                const WideNode w = load_wide(S.wide, node, tr.rp);
                 if (COUNT && active) rc.tc.nodes++;
                 float ee[4];
                 unsigned m = active ? slab4(w, tr.rp, tr.tmin, tr.t_best, ee) : 0u;
