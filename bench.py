@@ -283,7 +283,9 @@ def run_ours(args) -> None:
     # roofline of the dominant kernel (closest-hit traversal, wf_extend)
     kms = prof.kernel_ms
     dominant = max(("extend", "shade", "shadow", "generate", "accumulate"), key=lambda k: kms[k])
-    ext_launches = prof.kernel_launches and (prof.kernel_launches // max(1, 2 + 3 * st.pathtrace_bounces)) * st.pathtrace_bounces
+    # extend launches per frame: one per bounce and chunk of queue_capacity paths
+    chunk = st.queue_capacity if st.queue_capacity > 0 else paths_per_frame
+    ext_launches = -(-paths_per_frame // max(1, chunk)) * st.pathtrace_bounces
     per_ray_queue = 16 + 16 + 16 + 4 + 16            # ray o, d, state, queue slot; hit write
     wide_node_bytes = 7 * 16                         # 4-wide node: 6 planes x 4 boxes + refs
     alg_bytes = (cnt.ext_node_visits * wide_node_bytes + cnt.ext_leaf_bytes +
@@ -606,9 +608,10 @@ def run_profile_case(args) -> None:
     st.height //= args.profile_scale
     st.use_graph = False
     # the launch parameters the autotuner picks for this workload: one chunk,
-    # refill at 16 busy lanes, shadow work sorted by origin cell
+    # refill at 16 busy lanes, shadow work and extension rays sorted by
+    # origin cell (sort key 3)
     st.queue_capacity = st.width * st.height * st.samples ** 2
-    st.refill_below, st.sort_key = 16, 2
+    st.refill_below, st.sort_key = 16, 3
     st.engine = A.ENGINE_WAVEFRONT if args.profile_case == "wavefront" else A.ENGINE_MEGAKERNEL
     ctx = GpuContext(0)
     sid = ctx.upload(wl.scene)

@@ -884,6 +884,7 @@ struct WfScratch {
     WfJob* d_jobs = nullptr;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_key = 0;
+    unsigned long long last_key = 0;  // the shape of the previous frame
     SceneView graph_view0{};          // the parameters a one-scene graph was captured with
     WfJob graph_job0{};
     // second stream of a frame: bounce k's shadow kernel runs beside bounce
@@ -1044,8 +1045,10 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
     cudaError_t e = occupancy<COUNT, ONE>(occ);
     if (e != cudaSuccess) return e;
     const bool packet_first = ONE && W.args.packets != 0;
-    // timed (profiled) frames stay on one stream so that kernel classes add up
-    const bool overlap = W.side != nullptr && !lt.on;
+    // timed (profiled) frames stay on one stream so that kernel classes add
+    // up; chunks of under 2^20 paths too, whose kernels are shorter than the
+    // cross-stream waits would cost
+    const bool overlap = W.side != nullptr && !lt.on && Qeff >= (1 << 20);
     const WfArgs& A = W.args;
     const size_t smem = (size_t)kWfShared * kWfBlock * 8;
     // walk the path space in chunks of whole pixels
@@ -1250,9 +1253,17 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
                             : enqueue_frame<false, false>(W, jobs, iters, (int)Q, st, nl_out, lt));
     };
     if (lt.on) use_graph = false;
+    // a frame shape met for the first time runs as direct launches: a graph
+    // pays for its capture and instantiation only when the shape repeats
+    if (use_graph && !(W.graph && W.graph_key == key) && W.last_key != key) use_graph = false;
+    W.last_key = key;
     if (use_graph) {
         if (!W.graph || W.graph_key != key || !same_params) {
-            if (W.graph) { cudaGraphExecDestroy(W.graph); W.graph = nullptr; }
+            // same shape, another scene or job: the captured graph has the
+            // executable graph's topology, whose parameters are updated in
+            // place (no new instantiation)
+            const bool same_shape = W.graph && W.graph_key == key;
+            if (W.graph && !same_shape) { cudaGraphExecDestroy(W.graph); W.graph = nullptr; }
             cudaGraph_t g = nullptr;
             if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
                 return e;
@@ -1273,9 +1284,25 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
                 return ee;
             }
             if (e != cudaSuccess) return e;
-            e = cudaGraphInstantiate(&W.graph, g, 0);
+            bool updated = false;
+            if (same_shape) {
+                cudaGraphExecUpdateResultInfo info;
+                updated = cudaGraphExecUpdate(W.graph, g, &info) == cudaSuccess;
+                if (!updated) {
+                    (void)cudaGetLastError();
+                    cudaGraphExecDestroy(W.graph);
+                    W.graph = nullptr;
+                }
+            }
+            if (!updated) {
+                e = cudaGraphInstantiate(&W.graph, g, 0);
+                if (e != cudaSuccess) {
+                    cudaGraphDestroy(g);
+                    W.graph = nullptr;
+                    return e;
+                }
+            }
             cudaGraphDestroy(g);
-            if (e != cudaSuccess) { W.graph = nullptr; return e; }
             W.graph_key = key;
             W.graph_view0 = W.args.view0;
             W.graph_job0 = W.args.job0;

@@ -453,6 +453,15 @@ def test_full_size_sphere_cloud_properties(gpu):
     st = w.settings
     st.engine = A.ENGINE_WAVEFRONT
     wf = gpu.render(sid, st)
+    # the same frame again: a repeated frame shape runs as a CUDA graph in
+    # which each bounce's shadow kernel overlaps the next bounce's extend
+    # kernel on a second stream; the image is the same
+    for sort_key in (2, 3):
+        st.sort_key = sort_key
+        for _ in range(2):
+            again = gpu.render(sid, st)
+            assert np.array_equal(again.view(np.uint32), wf.view(np.uint32)), sort_key
+    st.sort_key = 0
     st.engine = A.ENGINE_MEGAKERNEL
     mk = gpu.render(sid, st)
     same8 = np.all(wf.view(np.uint32) == mk.view(np.uint32), axis=2).mean()
