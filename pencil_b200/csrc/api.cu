@@ -547,10 +547,11 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     idx.resize(n_nodes);
     int n_int = 0, n_leaf = 0;
     for (int k = 0; k < n_nodes; ++k) idx[k] = nodes[k].left < 0 ? n_leaf++ : n_int++;
-    // vertices: mesh vertices first, then those of explicit triangles
+    // triangles keep their three vertices in their leaf slot (geo_a, geo_b,
+    // geo_c): a triangle test then loads them directly, not via indices
     int n_explicit_tri = 0;
     for (int k = 0; k < s->n_prims; ++k) n_explicit_tri += s->prims[k].type == PGPU_PRIM_TRIANGLE;
-    const size_t n_verts = (size_t)s->n_mesh_vertices + 3 * (size_t)n_explicit_tri;
+    const bool has_tri = n_explicit_tri > 0 || s->n_mesh_triangles > 0;
 
     auto ref_of = [&](int k) -> int {
         if (nodes[k].left >= 0) return idx[k];
@@ -565,8 +566,9 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     size_t off_nodes = 0;
     size_t off_ga = align256(off_nodes + (size_t)n_int * 64);
     size_t off_gb = align256(off_ga + (size_t)n_leaf * 16);
-    size_t off_vt = align256(off_gb + (size_t)n_leaf * 16);
-    size_t off_lm = align256(off_vt + n_verts * 16);
+    size_t off_gc = align256(off_gb + (size_t)n_leaf * 16);
+    const size_t gc_bytes = has_tri ? (size_t)n_leaf * 16 : 0;
+    size_t off_lm = align256(off_gc + gc_bytes);
     size_t off_lp = align256(off_lm + (size_t)n_leaf * 4);
     size_t off_mt = align256(off_lp + (size_t)n_leaf * 4);
     size_t off_lt = align256(off_mt + (size_t)s->n_materials * sizeof(DevMaterial));
@@ -583,13 +585,13 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         c->stage_cap = total + wide_cap;
     }
     unsigned char* host = c->h_stage;
-    // every byte is written below except geo_b of one-word primitives and the
-    // alignment gaps; those are zeroed so that uploads are deterministic
+    // every byte is written below except the alignment gaps; those are
+    // zeroed so that uploads are deterministic
     {
         const size_t ends[][2] = {{off_nodes + (size_t)n_int * 64, off_ga},
                                   {off_ga + (size_t)n_leaf * 16, off_gb},
-                                  {off_gb, off_vt},
-                                  {off_vt + n_verts * 16, off_lm},
+                                  {off_gb + (size_t)n_leaf * 16, off_gc},
+                                  {off_gc + gc_bytes, off_lm},
                                   {off_lm + (size_t)n_leaf * 4, off_lp},
                                   {off_lp + (size_t)n_leaf * 4, off_mt},
                                   {off_mt + (size_t)s->n_materials * sizeof(DevMaterial), off_lt},
@@ -600,7 +602,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     float4* h_nodes = reinterpret_cast<float4*>(host + off_nodes);
     float4* h_ga = reinterpret_cast<float4*>(host + off_ga);
     float4* h_gb = reinterpret_cast<float4*>(host + off_gb);
-    float4* h_vt = reinterpret_cast<float4*>(host + off_vt);
+    float4* h_gc = has_tri ? reinterpret_cast<float4*>(host + off_gc) : nullptr;
     int* h_lm = reinterpret_cast<int*>(host + off_lm);
     int* h_lp = reinterpret_cast<int*>(host + off_lp);
     DevMaterial* h_mt = reinterpret_cast<DevMaterial*>(host + off_mt);
@@ -621,13 +623,11 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     });
     for (int m : quad_mats) h_mt[m].area_emitter = 1;
     if (!lights.empty()) std::memcpy(host + off_lt, lights.data(), lights.size() * sizeof(DevLight));
-    parallel_for(s->n_mesh_vertices, [&](int b, int e) {
-        for (int k = b; k < e; ++k)
-            h_vt[k] = make_float4(s->mesh_vertices[3 * k], s->mesh_vertices[3 * k + 1],
-                                  s->mesh_vertices[3 * k + 2], 0.0f);
-    });
-    size_t next_vert = (size_t)s->n_mesh_vertices;
-    // explicit triangles take vertices in DFS leaf order: sequential then
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    auto vertex = [&](int i) {
+        const float* v = s->mesh_vertices + 3 * (size_t)i;
+        return make_float4(v[0], v[1], v[2], 0.0f);
+    };
     auto convert = [&](int kb, int ke) {
     for (int k = kb; k < ke; ++k) {
         const pgpu_bvh_node& nd = nodes[k];
@@ -645,44 +645,44 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         const int slot = idx[k];
         const int prim = nd.right;
         h_lp[slot] = prim;
+        float4 a = zero, b = zero, c = zero;
         if (prim >= s->n_prims) {
-            int t = prim - s->n_prims;
+            const int t = prim - s->n_prims;
             h_lm[slot] = s->mesh_materials[t];
-            int4 tri = make_int4(s->mesh_indices[3 * t], s->mesh_indices[3 * t + 1],
-                                 s->mesh_indices[3 * t + 2], 0);
-            std::memcpy(&h_ga[slot], &tri, 16);
-            continue;
-        }
-        const pgpu_prim& p = s->prims[prim];
-        const float* q = p.p;
-        h_lm[slot] = p.material;
-        switch (p.type) {
-            case PGPU_PRIM_SPHERE:
-            case PGPU_PRIM_CUBE:
-                h_ga[slot] = make_float4(q[0], q[1], q[2], q[3]);
-                break;
-            case PGPU_PRIM_TRIANGLE: {
-                int base = (int)next_vert;
-                for (int v = 0; v < 3; ++v)
-                    h_vt[next_vert++] = make_float4(q[3 * v], q[3 * v + 1], q[3 * v + 2], 0.0f);
-                int4 tri = make_int4(base, base + 1, base + 2, 0);
-                std::memcpy(&h_ga[slot], &tri, 16);
-                break;
+            a = vertex(s->mesh_indices[3 * t]);
+            b = vertex(s->mesh_indices[3 * t + 1]);
+            c = vertex(s->mesh_indices[3 * t + 2]);
+        } else {
+            const pgpu_prim& p = s->prims[prim];
+            const float* q = p.p;
+            h_lm[slot] = p.material;
+            switch (p.type) {
+                case PGPU_PRIM_SPHERE:
+                case PGPU_PRIM_CUBE:
+                    a = make_float4(q[0], q[1], q[2], q[3]);
+                    break;
+                case PGPU_PRIM_TRIANGLE:
+                    a = make_float4(q[0], q[1], q[2], 0.0f);
+                    b = make_float4(q[3], q[4], q[5], 0.0f);
+                    c = make_float4(q[6], q[7], q[8], 0.0f);
+                    break;
+                case PGPU_PRIM_PLANE:
+                    a = make_float4(q[0], q[1], q[2], 0.0f);
+                    b = make_float4(q[3], q[4], q[5], 0.0f);
+                    break;
+                case PGPU_PRIM_CYLINDER:
+                case PGPU_PRIM_CONE:
+                    a = make_float4(q[0], q[1], q[2], q[6]);
+                    b = make_float4(q[3], q[4], q[5], q[7]);
+                    break;
             }
-            case PGPU_PRIM_PLANE:
-                h_ga[slot] = make_float4(q[0], q[1], q[2], 0.0f);
-                h_gb[slot] = make_float4(q[3], q[4], q[5], 0.0f);
-                break;
-            case PGPU_PRIM_CYLINDER:
-            case PGPU_PRIM_CONE:
-                h_ga[slot] = make_float4(q[0], q[1], q[2], q[6]);
-                h_gb[slot] = make_float4(q[3], q[4], q[5], q[7]);
-                break;
         }
+        h_ga[slot] = a;
+        h_gb[slot] = b;
+        if (h_gc) h_gc[slot] = c;
     }
     };
-    if (n_explicit_tri > 0) convert(0, n_nodes);
-    else parallel_for(n_nodes, convert);
+    parallel_for(n_nodes, convert);
 
     PGPU_CUDA(c, cudaSetDevice(c->device));
     auto ds = std::make_unique<DeviceScene>();
@@ -753,7 +753,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     v.wide = n_wide ? static_cast<const float4*>(ds->arena_wide) : nullptr;
     v.geo_a = reinterpret_cast<const float4*>(base + off_ga);
     v.geo_b = reinterpret_cast<const float4*>(base + off_gb);
-    v.verts = reinterpret_cast<const float4*>(base + off_vt);
+    v.geo_c = has_tri ? reinterpret_cast<const float4*>(base + off_gc) : nullptr;
     v.leaf_mat = reinterpret_cast<const int*>(base + off_lm);
     v.leaf_prim = reinterpret_cast<const int*>(base + off_lp);
     v.mats = reinterpret_cast<const DevMaterial*>(base + off_mt);

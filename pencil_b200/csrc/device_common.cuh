@@ -452,10 +452,9 @@ __device__ __forceinline__ bool hit_leaf(const SceneView& S, int ref, const Ray&
         case LEAF_SPHERE:
             return hit_sphere<REC>(ga, r, tmin, tmax, t, h);
         case LEAF_TRIANGLE: {
-            int i0 = __float_as_int(ga.x), i1 = __float_as_int(ga.y), i2 = __float_as_int(ga.z);
-            float4 a = __ldg(S.verts + i0), b = __ldg(S.verts + i1), c = __ldg(S.verts + i2);
-            return hit_triangle<REC>(v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), r,
-                                     tmin, tmax, t, h);
+            const float4 b = __ldg(S.geo_b + slot), c = __ldg(S.geo_c + slot);
+            return hit_triangle<REC>(v3(ga.x, ga.y, ga.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z),
+                                     r, tmin, tmax, t, h);
         }
         case LEAF_CUBE:
             return hit_cube<REC>(ga, r, tmin, tmax, t, h);
@@ -475,7 +474,7 @@ __device__ __forceinline__ int leaf_bytes(int ref) {
     int type = (~ref) >> kLeafTypeShift;
     switch (type) {
         case LEAF_SPHERE: case LEAF_CUBE: return 16;
-        case LEAF_TRIANGLE: return 16 + 3 * 16;
+        case LEAF_TRIANGLE: return 3 * 16;
         default: return 32;
     }
 }

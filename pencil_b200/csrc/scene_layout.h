@@ -21,16 +21,20 @@
 //             [8i+7]    = unused
 //   geo_a   float4[n_leaves]        leaf geometry in DFS leaf order (slot):
 //             sphere   (center.xyz, radius)
-//             triangle (i0, i1, i2, -)  int bits, indices into verts
+//             triangle (v0.xyz, -)
 //             cube     (center.xyz, half)
 //             plane    (point.xyz, -)
 //             cylinder (center.xyz, radius)
 //             cone     (apex.xyz, radius)
-//   geo_b   float4[n_leaves]        second word where needed:
+//   geo_b   float4[n_leaves]        second word where needed (zero elsewhere):
+//             triangle (v1.xyz, -)
 //             plane    (normal.xyz, -)
 //             cylinder (axis.xyz, half_height)
 //             cone     (axis.xyz, height)
-//   verts   float4[n_verts]         triangle vertices (xyz, -)
+//   geo_c   float4[n_leaves]        only in scenes with triangles:
+//             triangle (v2.xyz, -)
+//           (a triangle's vertices sit in its slot, so its test loads them
+//            at once instead of through an index word)
 //   leaf_mat  int32[n_leaves]       material id per slot
 //   leaf_prim int32[n_leaves]       caller's primitive index per slot
 //   mats    DevMaterial[n_materials]
@@ -95,7 +99,7 @@ struct SceneView {
     const float4* wide;    // 4-wide nodes (null when the root is a leaf)
     const float4* geo_a;
     const float4* geo_b;
-    const float4* verts;
+    const float4* geo_c;   // null in scenes without triangles
     const int* leaf_mat;
     const int* leaf_prim;
     const DevMaterial* mats;
