@@ -22,7 +22,7 @@ INCLUDE = HERE.parent / "include"
 
 CU_SOURCES = ["api.cu", "megakernel.cu", "wavefront.cu", "queries.cu", "adjoint.cu",
               "tonemap.cu", "bvh_device.cu"]
-CXX_SOURCES = ["bvh_build.cpp", "bvh_wide.cpp"]
+CXX_SOURCES = ["bvh_build.cpp", "bvh_wide.cpp", "host_pool.cpp"]
 HEADERS = ["device_common.cuh", "path.cuh", "scene_layout.h", "host_internal.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -13,7 +13,6 @@
 #include <map>
 #include <memory>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "host_internal.h"
@@ -66,7 +65,8 @@ struct DeviceScene {
     int n_wide = 0;
     int wide_stack = 0;
     int depth = 0;
-    std::vector<DevMaterial> mats;
+    int n_materials = 0;
+    bool has_glass = false;            // a dielectric material (two-branch glass needs it)
     std::vector<DevLight> lights;
     std::vector<int> quad_mats;        // material ids of quad-light emitters
     DevMaterial* d_mats = nullptr;
@@ -151,7 +151,6 @@ struct pgpu_ctx {
     std::vector<int2> ws_size_height;
     std::vector<char> ws_seen;
     WideScratch ws_collapse;
-    std::vector<DevMaterial> spare_mats;   // material table of the last freed scene
 };
 
 namespace {
@@ -172,22 +171,17 @@ int cuda_fail(pgpu_ctx* c, cudaError_t e, const char* what) {
     return fail(c, PGPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-// f(begin, end) over [0, n) on up to 16 host threads (one when n is small).
+// f(begin, end) over [0, n) on the host worker threads (one when n is small).
 template <class F>
 void parallel_for(int n, F f) {
     constexpr int kGrain = 16384;
-    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    const int T = std::min({16, hw, (n + kGrain - 1) / kGrain});
+    const int T = std::min(host_threads(), (n + kGrain - 1) / kGrain);
     if (T <= 1) { f(0, n); return; }
-    std::vector<std::thread> th;
-    th.reserve(T - 1);
     const int chunk = (n + T - 1) / T;
-    for (int t = 1; t < T; ++t) {
+    host_run(T, [&](int t) {
         const int b = t * chunk, e = std::min(n, b + chunk);
-        if (b < e) th.emplace_back([=] { f(b, e); });
-    }
-    f(0, std::min(n, chunk));
-    for (auto& x : th) x.join();
+        if (b < e) f(b, e);
+    });
 }
 
 // Smallest index in [0, n) for which bad(k) holds, or -1 (threads).
@@ -250,6 +244,21 @@ DeviceScene* find_scene(pgpu_ctx* c, int id) {
 // Validate Pencil's DFS node table against the unified primitive count:
 // node 0 is the root, an interior node's left child is the next node and its
 // right child comes later, every primitive is the leaf of exactly one node.
+// A caller's material as the device reads it (area_emitter is set apart,
+// from the scene's quad lights).
+DevMaterial dev_material(const pgpu_material& m) {
+    DevMaterial d{};
+    std::memcpy(d.albedo, m.albedo, 12);
+    d.kind = m.kind;
+    std::memcpy(d.emission, m.emission, 12);
+    d.reflectivity = m.reflectivity;
+    d.ior = m.ior;
+    d.specular = m.specular;
+    d.shininess = m.shininess;
+    std::memcpy(d.specular_color, m.specular_color, 12);
+    return d;
+}
+
 int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims, int& depth) {
     depth = 0;
     if (n_prims == 0) {
@@ -268,12 +277,17 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     // DFS pre-order (the order Pencil's recursive build emits): an interior
     // node k has its left subtree at k + 1 and its right subtree right after
     // the left one. Subtree sizes, from the back, check exactly that; the
-    // same sweep takes subtree heights (the root's is the depth) and checks
-    // that every primitive is in exactly one leaf.
+    // same sweep takes subtree heights (the root's is the depth), checks
+    // that every primitive is in exactly one leaf and numbers the interior
+    // nodes and the leaves in DFS order (c->ws_idx; counted from the back,
+    // as a valid table has n_prims leaves and n_prims - 1 interior nodes).
     std::vector<int2>& sh = c->ws_size_height;     // (subtree size, height)
     sh.resize(n_nodes);
+    std::vector<int>& idx = c->ws_idx;
+    idx.resize(n_nodes);
     std::vector<char>& seen = c->ws_seen;
     seen.assign(n_prims, 0);
+    int next_leaf = n_prims - 1, next_int = n_prims - 2;
     for (int k = n_nodes - 1; k >= 0; --k) {
         const pgpu_bvh_node& nd = nodes[k];
         if (nd.left < 0) {
@@ -282,8 +296,10 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
             if (seen[nd.right]++)
                 return fail(c, PGPU_ERR_BVH_INVALID, "primitive %d is in two leaves", nd.right);
             sh[k] = make_int2(1, 1);
+            idx[k] = next_leaf--;
             continue;
         }
+        idx[k] = next_int--;
         if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes ||
             nd.right != nd.left + sh[nd.left].x)
             return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
@@ -542,16 +558,14 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     int rc = check_tree(c, nodes, n_nodes, nU, depth);
     if (rc) return rc;
 
-    // DFS order numbering: interior nodes and leaf slots
-    std::vector<int>& idx = c->ws_idx;
-    idx.resize(n_nodes);
-    int n_int = 0, n_leaf = 0;
-    for (int k = 0; k < n_nodes; ++k) idx[k] = nodes[k].left < 0 ? n_leaf++ : n_int++;
+    // DFS order numbering of interior nodes and leaf slots (check_tree)
+    const std::vector<int>& idx = c->ws_idx;
+    const int n_leaf = nU, n_int = nU > 0 ? nU - 1 : 0;
     // triangles keep their three vertices in their leaf slot (geo_a, geo_b,
     // geo_c): a triangle test then loads them directly, not via indices
-    int n_explicit_tri = 0;
-    for (int k = 0; k < s->n_prims; ++k) n_explicit_tri += s->prims[k].type == PGPU_PRIM_TRIANGLE;
-    const bool has_tri = n_explicit_tri > 0 || s->n_mesh_triangles > 0;
+    const bool has_tri = s->n_mesh_triangles > 0 || first_bad(s->n_prims, [&](int k) {
+        return s->prims[k].type == PGPU_PRIM_TRIANGLE;
+    }) >= 0;
 
     auto ref_of = [&](int k) -> int {
         if (nodes[k].left >= 0) return idx[k];
@@ -607,19 +621,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     int* h_lp = reinterpret_cast<int*>(host + off_lp);
     DevMaterial* h_mt = reinterpret_cast<DevMaterial*>(host + off_mt);
     parallel_for(s->n_materials, [&](int b, int e) {
-        for (int k = b; k < e; ++k) {
-            const pgpu_material& m = s->materials[k];
-            DevMaterial d{};
-            std::memcpy(d.albedo, m.albedo, 12);
-            d.kind = m.kind;
-            std::memcpy(d.emission, m.emission, 12);
-            d.reflectivity = m.reflectivity;
-            d.ior = m.ior;
-            d.specular = m.specular;
-            d.shininess = m.shininess;
-            std::memcpy(d.specular_color, m.specular_color, 12);
-            h_mt[k] = d;
-        }
+        for (int k = b; k < e; ++k) h_mt[k] = dev_material(s->materials[k]);
     });
     for (int m : quad_mats) h_mt[m].area_emitter = 1;
     if (!lights.empty()) std::memcpy(host + off_lt, lights.data(), lights.size() * sizeof(DevLight));
@@ -736,11 +738,10 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
             return cuda_fail(c, e, "scene upload");
         }
     }
-    // host copy of the material table (material updates, glass flag) while
-    // the copies run; the last freed scene's vector has its pages mapped
-    std::vector<DevMaterial> mats = std::move(c->spare_mats);
-    c->spare_mats = {};
-    mats.assign(h_mt, h_mt + s->n_materials);
+    // the glass flag while the copies run
+    const bool has_glass = first_bad(s->n_materials, [&](int k) {
+        return s->materials[k].kind == PGPU_MAT_DIELECTRIC;
+    }) >= 0;
     e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
         release();
@@ -777,7 +778,8 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     ds->n_wide = n_wide;
     ds->wide_stack = wide_stack;
     ds->depth = depth;
-    ds->mats = std::move(mats);
+    ds->n_materials = s->n_materials;
+    ds->has_glass = has_glass;
     ds->lights = std::move(lights);
     ds->quad_mats = std::move(quad_mats);
     ds->d_mats = reinterpret_cast<DevMaterial*>(base + off_mt);
@@ -796,7 +798,6 @@ int32_t pgpu_free_scene(pgpu_ctx* c, int32_t id) {
     cudaStreamSynchronize(c->stream);
     cudaFreeAsync(ds->arena, c->stream);
     if (ds->arena_wide) cudaFreeAsync(ds->arena_wide, c->stream);
-    if (ds->mats.capacity() > c->spare_mats.capacity()) c->spare_mats.swap(ds->mats);
     c->scenes.erase(id);
     return PGPU_OK;
 }
@@ -858,26 +859,21 @@ int32_t pgpu_update_materials(pgpu_ctx* c, int32_t id, const pgpu_material* m, i
     if (!c) return PGPU_ERR_INVALID_ARG;
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
-    if (!m || n != (int)ds->mats.size())
-        return fail(c, PGPU_ERR_INVALID_ARG, "material count %d, scene has %zu", n, ds->mats.size());
-    std::vector<DevMaterial> mats(ds->mats);
+    if (!m || n != ds->n_materials)
+        return fail(c, PGPU_ERR_INVALID_ARG, "material count %d, scene has %d", n, ds->n_materials);
+    std::vector<DevMaterial> mats(n);
+    bool has_glass = false;
     for (int k = 0; k < n; ++k) {
         if (m[k].kind < PGPU_MAT_DIFFUSE || m[k].kind > PGPU_MAT_DIELECTRIC || m[k].flags != 0)
             return fail(c, PGPU_ERR_UNSUPPORTED, "material %d unsupported", k);
-        DevMaterial& d = mats[k];
-        std::memcpy(d.albedo, m[k].albedo, 12);
-        d.kind = m[k].kind;
-        std::memcpy(d.emission, m[k].emission, 12);
-        d.reflectivity = m[k].reflectivity;
-        d.ior = m[k].ior;
-        d.specular = m[k].specular;
-        d.shininess = m[k].shininess;
-        std::memcpy(d.specular_color, m[k].specular_color, 12);
+        mats[k] = dev_material(m[k]);
+        has_glass = has_glass || m[k].kind == PGPU_MAT_DIELECTRIC;
     }
+    for (int q : ds->quad_mats) mats[q].area_emitter = 1;
     PGPU_CUDA(c, cudaMemcpyAsync(ds->d_mats, mats.data(), mats.size() * sizeof(DevMaterial),
                                  cudaMemcpyHostToDevice, c->stream));
     PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-    ds->mats = mats;
+    ds->has_glass = has_glass;
     return PGPU_OK;
 }
 
@@ -1177,7 +1173,7 @@ int32_t pgpu_adjoint(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, const
         return fail(c, PGPU_ERR_UNSUPPORTED, "adjoint supports at most %d lights", adjoint_max_lights());
     PGPU_CUDA(c, cudaSetDevice(c->device));
     const size_t n3 = (size_t)cfg.W * cfg.H * 3;
-    const size_t nm = ds->mats.size(), nl = ds->lights.size();
+    const size_t nm = (size_t)ds->n_materials, nl = ds->lights.size();
     const size_t grad_b = (2 * nm + nl) * 3 * sizeof(double);
     const size_t need = align256(n3 * 4) + align256(n3 * 4) + align256(grad_b);
     if ((rc = ensure(c, c->d_adj, c->adj_cap, need))) return rc;
@@ -1278,8 +1274,7 @@ extern "C" int32_t pgpu_render_noalloc(pgpu_ctx* c, int32_t id, const pgpu_rende
     PGPU_CUDA(c, cudaSetDevice(c->device));
     const char* why = nullptr;
     int launches = 0;
-    bool has_glass = false;
-    for (const auto& m : ds->mats) has_glass = has_glass || m.kind == PGPU_MAT_DIELECTRIC;
+    const bool has_glass = ds->has_glass;
     *c->h_status = 0;
     cudaError_t e = wavefront_render_static(c->device, ds->view, ds->lights.data(),
                                             (int)ds->lights.size(), has_glass, cfg, out_rgb_device,

@@ -16,8 +16,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <atomic>
-#include <thread>
 #include <vector>
 
 #include <vector_functions.h>
@@ -49,26 +47,16 @@ void write_node(float4* q, const float (&lo)[3][4], const float (&hi)[3][4], con
 // (local indices) shifted by base[t].
 void parallel_relocate(float4* out, const std::vector<std::vector<float4>>& local,
                        const std::vector<int>& count, const std::vector<int>& base) {
-    const int n = (int)count.size();
-    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    const int T = std::max(1, std::min({16, hw, n}));
-    std::atomic<int> next{0};
-    auto worker = [&] {
-        for (int t; (t = next.fetch_add(1)) < n;) {
-            const int cnt = count[t];
-            float4* dst = out + (size_t)base[t] * kWideNodeFloat4;
-            std::copy_n(local[t].begin(), (size_t)cnt * kWideNodeFloat4, dst);
-            for (int w = 0; w < cnt; ++w) {
-                int* refs = reinterpret_cast<int*>(dst + (size_t)w * kWideNodeFloat4 + 6);
-                for (int k = 0; k < 4; ++k)
-                    if (refs[k] >= 0) refs[k] += base[t];
-            }
+    host_run((int)count.size(), [&](int t) {
+        const int cnt = count[t];
+        float4* dst = out + (size_t)base[t] * kWideNodeFloat4;
+        std::copy_n(local[t].begin(), (size_t)cnt * kWideNodeFloat4, dst);
+        for (int w = 0; w < cnt; ++w) {
+            int* refs = reinterpret_cast<int*>(dst + (size_t)w * kWideNodeFloat4 + 6);
+            for (int k = 0; k < 4; ++k)
+                if (refs[k] >= 0) refs[k] += base[t];
         }
-    };
-    std::vector<std::thread> th;
-    for (int k = 1; k < T; ++k) th.emplace_back(worker);
-    worker();
-    for (auto& x : th) x.join();
+    });
 }
 
 struct Collapser {
@@ -197,14 +185,10 @@ int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_r
         c.build(todo[head + t].binary, local_need[t]);
         local_n[t] = c.n_wide;
     };
-    {
-        std::vector<std::thread> th;
-        std::atomic<int> next{0};
-        auto worker = [&] { for (int t; (t = next.fetch_add(1)) < n_tasks;) run(t); };
-        const int nt = std::min(T, std::max(1, n_tasks));
-        for (int k = 1; k < nt; ++k) th.emplace_back(worker);
-        worker();
-        for (auto& x : th) x.join();
+    if (T > 1) {
+        host_run(n_tasks, run);
+    } else {
+        for (int t = 0; t < n_tasks; ++t) run(t);
     }
     // layout: top nodes, then each task's block
     std::vector<int> base(n_tasks);
@@ -246,8 +230,7 @@ int collapse_wide(const pgpu_bvh_node* nodes, int n_nodes, const std::vector<int
     // greedy collapse; if a pathological tree would need a deeper stack than
     // the kernels hold, two children per node (the binary tree's own bound)
     // threads only pay off for large trees
-    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    const int threads = n_interior < 16384 ? 1 : std::min(16, hw);
+    const int threads = n_interior < 16384 ? 1 : host_threads();
     int n_wide = 0;
     for (int pass = 0; pass < 2; ++pass) {
         n_wide = collapse_parallel(nodes, leaf_ref, pass == 0, threads, out, scratch, stack_need);

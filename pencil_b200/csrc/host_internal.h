@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 #include "../../include/pencil_gpu.h"
@@ -16,6 +17,12 @@ void build_bvh(const std::vector<pgpu_prim>& prims, std::vector<pgpu_bvh_node>& 
                int& depth);
 int make_prim(int type, int material, const float* a, const float* b, const float* c, float s0,
               float s1, pgpu_prim* out);
+
+// host_pool.cpp: task(0 .. n-1) on the process's host worker threads and the
+// calling thread (up to 16 in all, started once); returns when every task
+// has run. Tasks must not call host_run themselves.
+int host_threads();
+void host_run(int n, const std::function<void(int)>& task);
 
 // Scratch memory of collapse_wide, kept by the caller between calls so that
 // repeated uploads reuse it instead of faulting in fresh pages.
