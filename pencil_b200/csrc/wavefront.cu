@@ -91,13 +91,13 @@ struct WfArgs {
                               // this many of its lanes are still traversing
     // sort keys 2/3 (counting sort by sort_key_of of each iteration's shadow
     // work, and with key 3 of its next extension rays):
-    int* key_s;               // [slot] key of the slot's first shadow ray
+    int* key_s;               // [e] key of tmp_s[e]'s first shadow ray
     int* tmp_s;               // unsorted slots with shadow work
     int* qs;                  // the same slots sorted by key
     int* hist_s;              // kSortBins counters, then local bin offsets
     int* chunk_off;           // kSortBins / 1024 chunk totals, then chunk offsets
     int* tcnt;                // [iteration * 2 + 1] slots with shadow work
-    int* key_e;               // [slot] key of the path's next extension ray
+    int* key_e;               // [e] key of the next queue's entry e
     int* qe;                  // the next queue sorted by key (shade keeps the
                               // unsorted one: it reads path state by slot)
     int* hist_e;
@@ -346,15 +346,20 @@ wf_extend(WfArgs A, int it) {
     flush_counts<COUNT>(A, rc, 1);
 }
 
-// Warp-aggregated append of `slot` where `take`: one atomic per warp.
+// Warp-aggregated append of `slot` where `take`: one atomic per warp; with
+// `keys`, `key` is stored at the same position.
 __device__ __forceinline__ void warp_append(bool take, int slot, int* counter, int* list,
-                                            int lane) {
+                                            int lane, int* keys = nullptr, int key = 0) {
     const unsigned m = __ballot_sync(0xffffffffu, take);
     if (!m) return;
     int first = 0;
     if (lane == __ffs(m) - 1) first = atomicAdd(counter, __popc(m));
     first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
-    if (take) list[first + __popc(m & ((1u << lane) - 1u))] = slot;
+    if (take) {
+        const int pos = first + __popc(m & ((1u << lane) - 1u));
+        list[pos] = slot;
+        if (keys) keys[pos] = key;
+    }
 }
 
 // ---- extend, camera rays of one scene: warp packets ------------------------------
@@ -541,10 +546,7 @@ wf_shade(WfArgs A, int it) {
             alive = shade_vertex(S, J.P, ps, found, h, E);
             E.store();
             shadow_work = E.kind != 0;
-            if (A.sort_key >= 2 && shadow_work) {
-                key = sort_key_of(S, E.o0, E.d0);
-                A.key_s[slot] = key;
-            }
+            if (A.sort_key >= 2 && shadow_work) key = sort_key_of(S, E.o0, E.d0);
             if (COUNT && alive && (ps.flags & kFlagWhitted)) rc.ref++;
             A.L[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, 0.0f);
             if (alive) {
@@ -555,16 +557,13 @@ wf_shade(WfArgs A, int it) {
                 if (A.sort_key == 1)
                     bin = (ps.ray.d.x < 0.0f ? 1 : 0) | (ps.ray.d.y < 0.0f ? 2 : 0) |
                           (ps.ray.d.z < 0.0f ? 4 : 0);
-                if (A.sort_key == 3) {
-                    key_next = sort_key_of<kMortonBitsE>(S, ps.ray.o, ps.ray.d);
-                    A.key_e[slot] = key_next;
-                }
+                if (A.sort_key == 3) key_next = sort_key_of<kMortonBitsE>(S, ps.ray.o, ps.ray.d);
             }
         }
-        // sort key 2: the unsorted list of slots with shadow work, ordered by
-        // wf_sort_scatter
+        // sort key 2: the unsorted list of slots with shadow work and their
+        // keys, ordered by wf_sort_scatter
         if (A.sort_key >= 2) {
-            warp_append(shadow_work, slot, A.tcnt + 2 * it + 1, A.tmp_s, lane);
+            warp_append(shadow_work, slot, A.tcnt + 2 * it + 1, A.tmp_s, lane, A.key_s, key);
             // bin counts, one atomic per distinct key in the warp
             const unsigned same = __match_any_sync(0xffffffffu, key);
             if (shadow_work && lane == __ffs(same) - 1) atomicAdd(A.hist_s + key, __popc(same));
@@ -582,7 +581,11 @@ wf_shade(WfArgs A, int it) {
             int first = 0;
             if (lane == __ffs(m) - 1) first = atomicAdd(cout + b, __popc(m));
             first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
-            if (alive && bin == b) qout[b * A.Q + first + __popc(m & ((1u << lane) - 1u))] = slot;
+            if (alive && bin == b) {
+                const int pos = first + __popc(m & ((1u << lane) - 1u));
+                qout[b * A.Q + pos] = slot;
+                if (A.sort_key == 3) A.key_e[pos] = key_next;   // one bin under key 3
+            }
         }
     }
     flush_counts<COUNT>(A, rc);
@@ -658,7 +661,7 @@ __global__ void __launch_bounds__(kSortChunk) wf_sort_chunks(int* chunk_off) {
 
 // Places every listed slot at its bin's next position (the order inside a
 // bin is arbitrary; a path's result does not depend on its queue position).
-// list[0, *count) -> out by key[slot].
+// list[0, *count) -> out by keyof[e], the key stored beside list entry e.
 __global__ void __launch_bounds__(kWfBlock)
 wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
                 const int* chunk_off, int* out) {
@@ -670,7 +673,7 @@ wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
         const int e = e0 + lane;
         const bool on = e < ns;
         const int slot = on ? list[e] : -1;
-        const int key = on ? keyof[slot] : -1;
+        const int key = on ? keyof[e] : -1;
         const unsigned same = __match_any_sync(0xffffffffu, key);
         const int leader = __ffs(same) - 1;
         int base = 0;
