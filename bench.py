@@ -389,7 +389,10 @@ def run_ours(args) -> None:
 
 
 def _event_ms(stream, fn, reps: int) -> float:
+    """Mean ms of fn() over `reps` calls after two untimed ones (a repeated
+    frame shape runs as a CUDA graph from its second call on)."""
     import torch
+    fn()
     fn()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
