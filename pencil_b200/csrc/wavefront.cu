@@ -503,10 +503,10 @@ struct StoreNee {
     }
 };
 
-// At most 80 registers (6 blocks per SM): the shading state machine is
+// At most 72 registers (7 blocks per SM): the shading state machine is
 // latency-bound, and the extra resident warps pay for a few spilled words.
 template <bool COUNT, bool ONE>
-__global__ void __launch_bounds__(kWfBlock, 6)
+__global__ void __launch_bounds__(kWfBlock, 7)
 wf_shade(WfArgs A, int it) {
     RayCount rc = {};
     QView qv = qview(A, it);
