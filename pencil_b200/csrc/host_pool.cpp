@@ -10,6 +10,8 @@
 #include <thread>
 #include <vector>
 
+#include <unistd.h>
+
 #include "host_internal.h"
 
 namespace pgpu {
@@ -74,9 +76,18 @@ private:
 };
 
 HostPool& pool() {
-    // never destroyed: its threads sleep until the process ends
-    static HostPool* p = new HostPool(
-        std::max(0, std::min(16, (int)std::max(1u, std::thread::hardware_concurrency())) - 1));
+    // Never destroyed: its threads sleep until the process ends. A child made
+    // by fork() has none of its parent's threads, so it starts its own pool
+    // (the parent's object is left as it is).
+    static std::mutex mu;
+    static HostPool* p = nullptr;
+    static pid_t owner = 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!p || owner != getpid()) {
+        p = new HostPool(
+            std::max(0, std::min(16, (int)std::max(1u, std::thread::hardware_concurrency())) - 1));
+        owner = getpid();
+    }
     return *p;
 }
 
