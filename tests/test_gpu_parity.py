@@ -290,7 +290,22 @@ def test_quad_light_box_matches_oracle(gpu):
     ref, _, _ = O.Oracle(w.scene).render_split(w.settings)
     near_exact(gpu.render(sid, w.settings), ref)
     w.settings.engine = A.ENGINE_MEGAKERNEL
-    near_exact(gpu.render(sid, w.settings), ref)
+    mk = gpu.render(sid, w.settings)
+    near_exact(mk, ref)
+    # pgpu_update_materials rebuilds the device table from the caller's
+    # records and keeps the quad light's emitter flag: the same table gives
+    # the same image, a changed albedo the image of a fresh upload with it
+    mats = w.scene.material_array().copy()
+    gpu.update_materials(sid, mats)
+    assert np.array_equal(gpu.render(sid, w.settings).view(np.uint32), mk.view(np.uint32))
+    mats["albedo"] *= np.float32(0.9)
+    gpu.update_materials(sid, mats)
+    changed = gpu.render(sid, w.settings)
+    w.scene.set_material_array(mats)
+    sid2 = gpu.upload(w.scene)
+    assert np.array_equal(changed.view(np.uint32), gpu.render(sid2, w.settings).view(np.uint32))
+    assert not np.array_equal(changed, mk)
+    gpu.free(sid2)
     gpu.free(sid)
 
 
