@@ -59,8 +59,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint, batch and image-quality measurements")
-    ap.add_argument("--profile-case", choices=["wavefront", "megakernel", "adjoint", "lbvh",
-                                               "tonemap"], default=None,
+    ap.add_argument("--profile-case", choices=["wavefront", "megakernel", "mesh", "adjoint",
+                                               "lbvh", "tonemap"], default=None,
                     help="render the workload once, kernels launched one by one (for ncu)")
     ap.add_argument("--profile-scale", type=int, default=1,
                     help="divide the image width and height by this (smaller ncu cases)")
@@ -605,19 +605,24 @@ def run_profile_case(args) -> None:
         print(json.dumps(out))
         ctx.close()
         return
-    wl = W.sphere_cloud()
+    mesh = args.profile_case == "mesh"
+    wl = W.mesh_box() if mesh else W.sphere_cloud()
     st = wl.settings
     st.width //= args.profile_scale
     st.height //= args.profile_scale
     st.use_graph = False
-    # the launch parameters the autotuner picks for this workload: one chunk,
-    # refill at 16 busy lanes, shadow work and extension rays sorted by
-    # origin cell (sort key 3)
-    st.queue_capacity = st.width * st.height * st.samples ** 2
-    st.refill_below, st.sort_key = 16, 3
-    st.engine = A.ENGINE_WAVEFRONT if args.profile_case == "wavefront" else A.ENGINE_MEGAKERNEL
+    # the launch parameters the autotuner picks for the workload: sphere
+    # cloud one chunk, refill at 16 busy lanes; mesh chunks of 2^24 paths,
+    # refill at 20; shadow work and extension rays sorted by origin cell
+    # (sort key 3)
+    if mesh:
+        st.queue_capacity, st.refill_below = 1 << 24, 20
+    else:
+        st.queue_capacity, st.refill_below = st.width * st.height * st.samples ** 2, 16
+    st.sort_key = 3
+    st.engine = A.ENGINE_MEGAKERNEL if args.profile_case == "megakernel" else A.ENGINE_WAVEFRONT
     ctx = GpuContext(0)
-    sid = ctx.upload(wl.scene)
+    sid = ctx.upload(wl.scene, wl.scene.build_bvh()[0] if mesh else None)
     stats = RenderStats()
     img = ctx.render(sid, st, stats=stats)
     assert np.isfinite(img).all()
