@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PGPU_ABI_VERSION 1
+#define PGPU_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 enum pgpu_status {
@@ -211,9 +211,13 @@ enum pgpu_flags {
                                      NO_GRAPH); see pgpu_stats.kernel_ms     */
     PGPU_FLAG_NO_PACKETS    = 32, /* wavefront: trace camera rays one per lane
                                      instead of as warp packets              */
-    PGPU_FLAG_MIS           = 64  /* path tracing with trace_path_mis's light
+    PGPU_FLAG_MIS           = 64, /* path tracing with trace_path_mis's light
                                      weights (RenderSettings::mis,
                                      src/renderer.hpp:55, 1205-1346)         */
+    PGPU_FLAG_BINARY_TREE   = 128 /* megakernel: traverse Pencil's binary tree
+                                     (src/bvh.hpp:31-48) instead of the 4-wide
+                                     tree collapsed from it, which both
+                                     engines use by default                  */
 };
 
 typedef struct pgpu_render_params {
@@ -238,6 +242,8 @@ typedef struct pgpu_render_params {
                                    by direction octant, 2 shadow work sorted
                                    by origin (Morton code) and octant, 3 also
                                    the extension rays of bounces >= 1        */
+    int32_t  block_size;        /* wavefront threads per block: 64, 128 or 256
+                                   (0: 128; pgpu_render_noalloc always 128)  */
 } pgpu_render_params;
 
 typedef struct pgpu_stats {
@@ -390,10 +396,14 @@ int32_t pgpu_adjoint(pgpu_ctx* ctx, int32_t scene_id,
  *
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) and reserves the context's error-message buffer;
- * make that first call before any stream capture. Every call shares the one
- * array and leaves its contents behind (each call clears what it reads
- * before it is written); calls that overlap on the GPU -- from two contexts
- * or two streams at once -- race on it and must be serialized. */
+ * make that first call before any stream capture. The address is kept for
+ * the life of the process, so do not cudaDeviceReset a device while the
+ * library is in use on it. Each call synchronizes its stream before it
+ * returns, and a call made while that stream is being captured is refused
+ * (PGPU_ERR_INVALID_ARG). Every call shares the one array and leaves its
+ * contents behind (each call clears what it reads before it is written);
+ * calls that overlap on the GPU -- from two contexts or two streams at
+ * once -- race on it and must be serialized. */
 int32_t pgpu_render_noalloc(pgpu_ctx* ctx, int32_t scene_id,
                             const pgpu_render_params* params,
                             float* out_rgb_device, float* out_m2_device);

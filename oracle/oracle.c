@@ -623,9 +623,10 @@ static v3 trace_path(ctx_t* c, ray_t r, int bounces, rng_t* rng) {
 typedef struct {
     const orc_scene* s;
     const pgpu_render_params* p;
-    float* out;
+    float* out;          /* the window's pixels, row-major */
     float* m2;
-    int row0, stride;    /* rows row0, row0 + stride, ... */
+    int x0, y0, ww, wh;  /* window of the image: pixels [x0, x0+ww) x [y0, y0+wh) */
+    int row0, stride;    /* window rows row0, row0 + stride, ... */
     uint64_t cnt[ORC_CNT_N];
 } job_t;
 
@@ -649,7 +650,7 @@ static void render_pixel(const job_t* jb, ctx_t* c, int i, int j) {
         }
     }
     acc = divf(acc, (float)(n * n));
-    size_t o = ((size_t)j * W + i) * 3;
+    size_t o = ((size_t)(j - jb->y0) * jb->ww + (i - jb->x0)) * 3;
     jb->out[o + 0] = acc.x; jb->out[o + 1] = acc.y; jb->out[o + 2] = acc.z;
     if (jb->m2) {
         sq = divf(sq, (float)(n * n));
@@ -665,22 +666,40 @@ static void* render_thread(void* arg) {
     c.cnt = jb->cnt;
     c.tv.s = jb->s;
     c.tv.cnt = jb->cnt;
-    for (int j = jb->row0; j < jb->p->height; j += jb->stride)
-        for (int i = 0; i < jb->p->width; ++i) render_pixel(jb, &c, i, j);
+    for (int j = jb->row0; j < jb->wh; j += jb->stride)
+        for (int i = 0; i < jb->ww; ++i) render_pixel(jb, &c, jb->x0 + i, jb->y0 + j);
     return NULL;
+}
+
+/* A window of the image, checked against the image size; NULL: all of it. */
+static int window_of(const pgpu_render_params* p, const int32_t* win, int w[4]) {
+    if (!win) { w[0] = 0; w[1] = 0; w[2] = p->width; w[3] = p->height; return 0; }
+    for (int k = 0; k < 4; ++k) w[k] = win[k];
+    if (w[0] < 0 || w[1] < 0 || w[2] <= 0 || w[3] <= 0 || w[0] + w[2] > p->width ||
+        w[1] + w[3] > p->height)
+        return -1;
+    return 0;
 }
 
 int32_t orc_render(const orc_scene* s, const pgpu_render_params* p, float* out_rgb,
                    float* out_m2, int32_t n_threads, uint64_t* counters) {
+    return orc_render_window(s, p, NULL, out_rgb, out_m2, n_threads, counters);
+}
+
+int32_t orc_render_window(const orc_scene* s, const pgpu_render_params* p, const int32_t* win,
+                          float* out_rgb, float* out_m2, int32_t n_threads, uint64_t* counters) {
     if (!s || !p || !out_rgb || p->width <= 0 || p->height <= 0 || p->samples <= 0) return -1;
     if (p->mode != PGPU_MODE_PATHTRACE && p->mode != PGPU_MODE_WHITTED) return -1;
+    int w[4];
+    if (window_of(p, win, w)) return -1;
     if (n_threads < 1) n_threads = 1;
-    if (n_threads > p->height) n_threads = p->height;
+    if (n_threads > w[3]) n_threads = w[3];
     job_t* jobs = (job_t*)calloc((size_t)n_threads, sizeof(job_t));
     pthread_t* th = (pthread_t*)calloc((size_t)n_threads, sizeof(pthread_t));
     char* live = (char*)calloc((size_t)n_threads, 1);
     for (int k = 0; k < n_threads; ++k) {
         jobs[k].s = s; jobs[k].p = p; jobs[k].out = out_rgb; jobs[k].m2 = out_m2;
+        jobs[k].x0 = w[0]; jobs[k].y0 = w[1]; jobs[k].ww = w[2]; jobs[k].wh = w[3];
         jobs[k].row0 = k; jobs[k].stride = n_threads;
     }
     for (int k = 1; k < n_threads; ++k)
@@ -982,9 +1001,10 @@ static v3 split_sample(split_t* sp, ray_t r, rng_t* rng) {
 typedef struct {
     const orc_scene* s;
     const pgpu_render_params* p;
-    float* out;
+    float* out;          /* the window's pixels, row-major */
     float* m2;
-    int row0, stride;
+    int x0, y0, ww, wh;  /* window of the image */
+    int row0, stride;    /* window rows row0, row0 + stride, ... */
     const char* area_emitter;
     const float* quad_area;
     int has_quad;
@@ -1000,8 +1020,9 @@ static void* split_thread(void* arg) {
     const int W = p->width, H = p->height, n = p->samples, spp = n * n;
     int G = 1;
     while (G * 2 <= (spp < 32 ? spp : 32)) G *= 2;
-    for (int j = jb->row0; j < H; j += jb->stride) {
-        for (int i = 0; i < W; ++i) {
+    for (int jw = jb->row0; jw < jb->wh; jw += jb->stride) {
+        const int j = jb->y0 + jw;
+        for (int i = jb->x0; i < jb->x0 + jb->ww; ++i) {
             v3 acc[32], acc2[32];
             for (int g = 0; g < G; ++g) {
                 acc[g] = mk(0, 0, 0);
@@ -1022,7 +1043,7 @@ static void* split_thread(void* arg) {
                     acc[g] = add(acc[g], acc[g + off]);
                     acc2[g] = add(acc2[g], acc2[g + off]);
                 }
-            size_t o = ((size_t)j * W + i) * 3;
+            size_t o = ((size_t)jw * jb->ww + (i - jb->x0)) * 3;
             jb->out[o + 0] = acc[0].x / (float)spp;
             jb->out[o + 1] = acc[0].y / (float)spp;
             jb->out[o + 2] = acc[0].z / (float)spp;
@@ -1038,7 +1059,15 @@ static void* split_thread(void* arg) {
 
 int32_t orc_render_split(const orc_scene* s, const pgpu_render_params* p, float* out_rgb,
                          float* out_m2, int32_t n_threads, uint64_t* counters) {
+    return orc_render_split_window(s, p, NULL, out_rgb, out_m2, n_threads, counters);
+}
+
+int32_t orc_render_split_window(const orc_scene* s, const pgpu_render_params* p,
+                                const int32_t* win, float* out_rgb, float* out_m2,
+                                int32_t n_threads, uint64_t* counters) {
     if (!s || !p || !out_rgb || p->width <= 0 || p->height <= 0 || p->samples <= 0) return -1;
+    int w[4];
+    if (window_of(p, win, w)) return -1;
     char* area_emitter = (char*)calloc((size_t)(s->n_materials > 0 ? s->n_materials : 1), 1);
     float* quad_area = (float*)calloc((size_t)(s->n_lights > 0 ? s->n_lights : 1), sizeof(float));
     int has_quad = 0;
@@ -1051,13 +1080,14 @@ int32_t orc_render_split(const orc_scene* s, const pgpu_render_params* p, float*
         has_quad = 1;
     }
     if (n_threads < 1) n_threads = 1;
-    if (n_threads > p->height) n_threads = p->height;
+    if (n_threads > w[3]) n_threads = w[3];
     sjob_t* jobs = (sjob_t*)calloc((size_t)n_threads, sizeof(sjob_t));
     pthread_t* th = (pthread_t*)calloc((size_t)n_threads, sizeof(pthread_t));
     char* live = (char*)calloc((size_t)n_threads, 1);
     for (int k = 0; k < n_threads; ++k) {
         sjob_t* jb = &jobs[k];
         jb->s = s; jb->p = p; jb->out = out_rgb; jb->m2 = out_m2;
+        jb->x0 = w[0]; jb->y0 = w[1]; jb->ww = w[2]; jb->wh = w[3];
         jb->row0 = k; jb->stride = n_threads;
         jb->area_emitter = area_emitter; jb->quad_area = quad_area; jb->has_quad = has_quad;
     }

@@ -72,6 +72,16 @@ int32_t orc_render_split(const orc_scene* s, const pgpu_render_params* p,
                          float* out_rgb, float* out_m2, int32_t n_threads,
                          uint64_t* counters);
 
+/* The same two renders restricted to a window win = {x, y, w, h} of the
+ * image p describes (pixels keep their full-image seeds and jitter);
+ * out_rgb / out_m2 hold the window's w*h*3 floats, row-major. */
+int32_t orc_render_window(const orc_scene* s, const pgpu_render_params* p,
+                          const int32_t* win, float* out_rgb, float* out_m2,
+                          int32_t n_threads, uint64_t* counters);
+int32_t orc_render_split_window(const orc_scene* s, const pgpu_render_params* p,
+                                const int32_t* win, float* out_rgb, float* out_m2,
+                                int32_t n_threads, uint64_t* counters);
+
 /* FP64 adjoint of the production estimator (test-only): replays each path
  * with the float32 geometry and decisions of orc_render_split and
  * accumulates, in double, dLoss/d(albedo), dLoss/d(emission) (3 per

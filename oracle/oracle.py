@@ -57,6 +57,10 @@ def load():
     lib.orc_render.restype = C.c_int32
     lib.orc_render_split.argtypes = lib.orc_render.argtypes
     lib.orc_render_split.restype = C.c_int32
+    for fn in (lib.orc_render_window, lib.orc_render_split_window):
+        fn.argtypes = [C.POINTER(OrcScene), C.POINTER(A.RenderParams), C.c_void_p, C.c_void_p,
+                       C.c_void_p, C.c_int32, C.c_void_p]
+        fn.restype = C.c_int32
     lib.orc_adjoint.argtypes = [C.POINTER(OrcScene), C.POINTER(A.RenderParams), C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
     lib.orc_adjoint.restype = C.c_int32
@@ -105,29 +109,31 @@ class Oracle:
         self.s = s
         self.basis = basis
 
-    def render(self, settings, threads: int | None = None, want_m2: bool = False):
+    def _render(self, fn, settings, threads, want_m2, window):
         p = settings.params()
-        out = np.zeros((settings.height, settings.width, 3), np.float32)
+        x, y, w, h = window if window is not None else (0, 0, settings.width, settings.height)
+        out = np.zeros((h, w, 3), np.float32)
         m2 = np.zeros_like(out) if want_m2 else None
         cnt = np.zeros(5, np.uint64)
-        rc = self.lib.orc_render(C.byref(self.s), C.byref(p), A.ptr(out), A.ptr(m2),
-                                 threads or os.cpu_count() or 1, A.ptr(cnt))
+        win = np.asarray([x, y, w, h], np.int32)
+        rc = fn(C.byref(self.s), C.byref(p), A.ptr(win), A.ptr(out), A.ptr(m2),
+                threads or os.cpu_count() or 1, A.ptr(cnt))
         if rc != 0:
-            raise ValueError("orc_render rejected its arguments")
+            raise ValueError(f"{fn.__name__} rejected its arguments")
         return out, m2, cnt
 
-    def render_split(self, settings, threads: int | None = None, want_m2: bool = False):
+    def render(self, settings, threads: int | None = None, want_m2: bool = False,
+               window: tuple[int, int, int, int] | None = None):
+        """The reference algorithm (Pencil's per-pixel RNG, both dielectric
+        branches). window = (x, y, w, h): only those pixels of the image."""
+        return self._render(self.lib.orc_render_window, settings, threads, want_m2, window)
+
+    def render_split(self, settings, threads: int | None = None, want_m2: bool = False,
+                     window: tuple[int, int, int, int] | None = None):
         """The GPU core's production estimator (counter RNG, Fresnel-split
         glass, quad-light NEE) restated on the CPU."""
-        p = settings.params()
-        out = np.zeros((settings.height, settings.width, 3), np.float32)
-        m2 = np.zeros_like(out) if want_m2 else None
-        cnt = np.zeros(5, np.uint64)
-        rc = self.lib.orc_render_split(C.byref(self.s), C.byref(p), A.ptr(out), A.ptr(m2),
-                                       threads or os.cpu_count() or 1, A.ptr(cnt))
-        if rc != 0:
-            raise ValueError("orc_render_split rejected its arguments")
-        return out, m2, cnt
+        return self._render(self.lib.orc_render_split_window, settings, threads, want_m2,
+                            window)
 
     def render_tile(self, settings, x: int, y: int, w: int, h: int) -> np.ndarray:
         """The distributed worker's tile (render_tile) of the full image

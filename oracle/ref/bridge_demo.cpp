@@ -9,8 +9,8 @@
 //
 // Environment PENCIL_GPU_EXACT=1 selects Pencil's own random stream.
 // Private members are opened with "#define private public" in this
-// translation unit only, standing in for the friend declarations a Pencil
-// build adds.
+// translation unit only, standing in for the one friend declaration per
+// class (friend struct ::pencil_gpu::Access) that a Pencil build adds.
 #include <algorithm>
 #include <atomic>
 #include <chrono>

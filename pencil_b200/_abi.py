@@ -33,10 +33,12 @@ MODE_PATHTRACE, MODE_WHITTED = 0, 1
 ENGINE_WAVEFRONT, ENGINE_MEGAKERNEL = 0, 1
 RNG_COUNTER, RNG_PIXEL_SEQUENTIAL = 0, 1
 GLASS_FRESNEL_SPLIT, GLASS_BOTH_BRANCHES = 0, 1
+ABI_VERSION = 2   # PGPU_ABI_VERSION of include/pencil_gpu.h
 FLAG_DEVICE_OUTPUT, FLAG_COUNT_RAYS, FLAG_COUNT_NODES, FLAG_NO_GRAPH = 1, 2, 4, 8
 FLAG_PROFILE_KERNELS = 16
 FLAG_NO_PACKETS = 32
 FLAG_MIS = 64
+FLAG_BINARY_TREE = 128
 TONEMAP_NONE, TONEMAP_ACES, TONEMAP_REINHARD = 0, 1, 2
 TONEMAP_DEVICE_INPUT, TONEMAP_DEVICE_OUTPUT = 1, 2
 KERNEL_CLASSES = ("generate", "extend", "shade", "shadow", "accumulate", "megakernel")
@@ -80,7 +82,7 @@ class RenderParams(C.Structure):
                 ("soft_shadow_samples", C.c_int32), ("seed", C.c_uint32),
                 ("sample_offset", C.c_int32), ("flags", C.c_int32),
                 ("queue_capacity", C.c_int32), ("refill_below", C.c_int32),
-                ("sort_key", C.c_int32)]
+                ("sort_key", C.c_int32), ("block_size", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -160,7 +162,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.pgpu_abi_version() != 1:
+    if lib.pgpu_abi_version() != ABI_VERSION:
         raise RuntimeError("libpencil_gpu.so ABI version mismatch")
     _lib = lib
     return lib

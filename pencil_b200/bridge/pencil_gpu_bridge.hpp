@@ -4,9 +4,10 @@
 // pencil::Renderer::render (src/renderer.hpp:198-295).
 //
 // Include it after Pencil's own headers in pencil.cpp. It reads stored fields
-// that Pencil keeps private; Pencil grants access with one line per class
-// (see INTEGRATION.md):  friend struct ::pencil_gpu::Access;
-// in Scene, BVH, Sphere, Triangle, Cube, Plane, Cylinder and Cone.
+// that Pencil keeps private; Pencil grants access with one line per class,
+//     friend struct ::pencil_gpu::Access;
+// in Scene, BVH, Sphere, Triangle, Cube, Plane, Cylinder and Cone, after a
+// forward declaration `namespace pencil_gpu { struct Access; }`.
 #pragma once
 
 #include <cstdlib>

@@ -930,6 +930,10 @@ int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, Re
     cfg.profile = (p->flags & PGPU_FLAG_PROFILE_KERNELS) != 0;
     cfg.packets = (p->flags & PGPU_FLAG_NO_PACKETS) == 0;
     cfg.mis = (p->flags & PGPU_FLAG_MIS) != 0;
+    cfg.binary_tree = (p->flags & PGPU_FLAG_BINARY_TREE) != 0;
+    if (p->block_size != 0 && p->block_size != 64 && p->block_size != 128 && p->block_size != 256)
+        return fail(c, PGPU_ERR_INVALID_ARG, "block_size must be 0, 64, 128 or 256");
+    cfg.block = p->block_size;
     (void)ds;
     return PGPU_OK;
 }
@@ -1272,6 +1276,13 @@ extern "C" int32_t pgpu_render_noalloc(pgpu_ctx* c, int32_t id, const pgpu_rende
     if (cfg.engine != PGPU_ENGINE_WAVEFRONT)
         return fail(c, PGPU_ERR_UNSUPPORTED, "the no-allocation render is the wavefront engine");
     PGPU_CUDA(c, cudaSetDevice(c->device));
+    // The call stages its scene view and job from host stack memory and
+    // synchronizes its stream before it returns; neither survives a capture.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PGPU_CUDA(c, cudaStreamIsCapturing(c->stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(c, PGPU_ERR_INVALID_ARG,
+                    "pgpu_render_noalloc was called while its stream is being captured");
     const char* why = nullptr;
     int launches = 0;
     const bool has_glass = ds->has_glass;

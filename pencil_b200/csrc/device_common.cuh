@@ -1011,6 +1011,31 @@ __device__ bool any_hit(const SceneView& S, const Ray& ray, float tmin, float tm
     }
 }
 
+// Closest hit / any hit of one ray on the 4-wide tree, traced to the end
+// (megakernel): the wavefront's resumable traversals run in one loop, so
+// both engines walk the same tree in the same order.
+template <int kShared, bool COUNT>
+__device__ __forceinline__ int closest_hit4(const SceneView& S, const Ray& ray, float tmin,
+                                            float tmax, float& t_best, int& best_ref,
+                                            TravStack<kShared>& stk, TravCount* cnt) {
+    ClosestTrav4<kShared, COUNT> tr;
+    if (!tr.init(S, ray, tmin, tmax, cnt))
+        while (!tr.step(S, stk, cnt)) {
+        }
+    t_best = tr.t_best;
+    best_ref = tr.best_ref;
+    return tr.best;
+}
+template <int kShared, bool COUNT>
+__device__ __forceinline__ bool any_hit4(const SceneView& S, const Ray& ray, float tmin,
+                                         float tmax, TravStack<kShared>& stk, TravCount* cnt) {
+    AnyTrav4<kShared, COUNT> tr;
+    if (!tr.init(S, ray, tmin, tmax, cnt))
+        while (!tr.step(S, stk, cnt)) {
+        }
+    return tr.hit;
+}
+
 // Full hit record of the closest hit found by closest_hit.
 __device__ __forceinline__ void make_hit(const SceneView& S, int best_ref, int slot,
                                          const Ray& ray, float tmin, float t_best, Hit& h) {

@@ -53,6 +53,8 @@ struct RenderCfg {
     bool profile;
     bool packets;     // wavefront: camera rays of a one-scene frame as warp packets
     bool mis;         // trace_path_mis's light weights
+    bool binary_tree; // megakernel: Pencil's binary tree instead of the 4-wide tree
+    int block;        // wavefront threads per block (0: the default)
 };
 
 // Device counters written by the kernels (atomic adds).

@@ -1,5 +1,8 @@
 // megakernel.cu - the plain GPU path tracer: one thread per (pixel, sample
 // lane), every bounce, shadow ray and the Whitted continuation in one kernel.
+// It traverses the same 4-wide tree as the wavefront by default (the
+// baseline the wavefront is measured against), or Pencil's binary tree with
+// PGPU_FLAG_BINARY_TREE.
 //
 // Thread mapping. Counter RNG: G = largest power of two <= min(spp, 32)
 // lanes share a pixel; lane g traces samples g, g + G, ... and the G partial
@@ -15,7 +18,7 @@ namespace pgpu {
 
 constexpr int kMkShared = 16;   // stack entries per thread kept in shared memory
 
-template <bool COUNT, bool TREE, bool PIXEL_SEQ>
+template <bool COUNT, bool TREE, bool PIXEL_SEQ, bool WIDE>
 __global__ void __launch_bounds__(128)
 mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __restrict__ m2,
           unsigned long long* __restrict__ counters) {
@@ -25,7 +28,7 @@ mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __re
     stk.st = reinterpret_cast<float*>(smem + kMkShared * blockDim.x) + threadIdx.x;
     stk.stride = blockDim.x;
     RayCount rc = {};
-    Tracer<kMkShared, COUNT> tr{S, P, stk, rc};
+    Tracer<kMkShared, COUNT, WIDE> tr{S, P, stk, rc};
 
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool tile = P.tile_w > 0;
@@ -92,15 +95,15 @@ mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __re
     }
 }
 
-template <bool COUNT, bool TREE, bool PIXEL_SEQ>
+template <bool COUNT, bool TREE, bool PIXEL_SEQ, bool WIDE>
 static cudaError_t launch_mk(const SceneView& S, const PathParams& P, int G, float* out,
                              float* m2, unsigned long long* counters, cudaStream_t st) {
     const int block = 128;
     long long threads = (P.tile_w > 0 ? (long long)P.tile_w * P.tile_h : (long long)P.W * P.H) * G;
     long long blocks = (threads + block - 1) / block;
     size_t smem = (size_t)kMkShared * block * 8;
-    mk_render<COUNT, TREE, PIXEL_SEQ><<<(unsigned)blocks, block, smem, st>>>(S, P, G, out, m2,
-                                                                               counters);
+    mk_render<COUNT, TREE, PIXEL_SEQ, WIDE><<<(unsigned)blocks, block, smem, st>>>(S, P, G, out,
+                                                                                     m2, counters);
     return cudaGetLastError();
 }
 
@@ -121,9 +124,11 @@ cudaError_t launch_megakernel(const SceneView& S, const RenderCfg& c, float* out
         int lim = c.spp < 32 ? c.spp : 32;
         while (G * 2 <= lim) G *= 2;
     }
-#define PGPU_MK_CASE(CNT, TR, SQ)                                          \
-    if (c.count == CNT && tree == TR && seq == SQ)                         \
-        return launch_mk<CNT, TR, SQ>(S, P, G, out, m2, counters, st);
+    const bool wide = !c.binary_tree;
+#define PGPU_MK_CASE(CNT, TR, SQ)                                                \
+    if (c.count == CNT && tree == TR && seq == SQ)                               \
+        return wide ? launch_mk<CNT, TR, SQ, true>(S, P, G, out, m2, counters, st) \
+                    : launch_mk<CNT, TR, SQ, false>(S, P, G, out, m2, counters, st);
     PGPU_MK_CASE(false, false, false)
     PGPU_MK_CASE(false, false, true)
     PGPU_MK_CASE(false, true, false)

@@ -326,7 +326,11 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& S, const PathParam
     return ps.depth > 0;
 }
 
-template <int kShared, bool COUNT>
+// One path traced to the end by one thread (megakernel). WIDE: traversal of
+// the 4-wide tree the wavefront walks (ClosestTrav4/AnyTrav4); otherwise
+// Pencil's binary tree (the tree BVHNode::hit walks, src/bvh.hpp:31-48) in
+// its child-pair layout, nearest child first.
+template <int kShared, bool COUNT, bool WIDE = false>
 struct Tracer {
     const SceneView& S;
     const PathParams& P;
@@ -337,13 +341,15 @@ struct Tracer {
         if (COUNT) rc.ext++;
         float tb;
         int bref;
-        int slot = closest_hit<kShared, COUNT>(S, r, 1e-4f, 1e9f, tb, bref, stk, &rc.tc);
+        int slot = WIDE ? closest_hit4<kShared, COUNT>(S, r, 1e-4f, 1e9f, tb, bref, stk, &rc.tc)
+                        : closest_hit<kShared, COUNT>(S, r, 1e-4f, 1e9f, tb, bref, stk, &rc.tc);
         if (slot >= 0) make_hit(S, bref, slot, r, 1e-4f, tb, h);
         return slot;
     }
     __device__ __forceinline__ bool occluded(const Ray& r, float tmin, float tmax) {
         if (COUNT) rc.shadow++;
-        return any_hit<kShared, COUNT>(S, r, tmin, tmax, stk, &rc.tc);
+        return WIDE ? any_hit4<kShared, COUNT>(S, r, tmin, tmax, stk, &rc.tc)
+                    : any_hit<kShared, COUNT>(S, r, tmin, tmax, stk, &rc.tc);
     }
 
     // Direct light of a Whitted vertex: emission + point/directional lights

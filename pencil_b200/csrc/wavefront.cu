@@ -35,7 +35,11 @@
 namespace pgpu {
 
 constexpr int kWfShared = 16;
+// Threads per block of the wavefront kernels: kWfBlock unless the render
+// asks for 64 or 256 (an autotuned launch shape); the kernels are compiled
+// for blocks of up to kWfMaxBlock threads.
 constexpr int kWfBlock = 128;
+constexpr int kWfMaxBlock = 256;
 constexpr int kOctants = 8;
 constexpr int kDefaultRefill = 20;   // lanes still busy when a warp refetches
 // Sort key 2: each iteration's shadow work ordered by the Morton code of the
@@ -233,7 +237,7 @@ __device__ __forceinline__ int fetch32(unsigned int* cursor) {
 
 // ---- generate -----------------------------------------------------------------
 template <bool COUNT, bool ONE>
-__global__ void __launch_bounds__(kWfBlock)
+__global__ void __launch_bounds__(kWfMaxBlock)
 wf_generate(WfArgs A, long long path_begin, int n_slots) {
     RayCount rc = {};
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -286,7 +290,7 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
 // lanes take new rays from the queue (one atomic per warp), so warps keep
 // traversing instead of waiting for their slowest ray.
 template <bool COUNT, bool ONE>
-__global__ void __launch_bounds__(kWfBlock)
+__global__ void __launch_bounds__(kWfMaxBlock)
 wf_extend(WfArgs A, int it) {
     extern __shared__ int smem[];
     TravStack<kWfShared> stk;
@@ -373,9 +377,9 @@ __device__ __forceinline__ void warp_append(bool take, int slot, int* counter, i
 // leaf only when its own slab test reaches it, so its result is the closest
 // hit among the same leaves as its own traversal would test.
 template <bool COUNT>
-__global__ void __launch_bounds__(kWfBlock) wf_extend_packet(WfArgs A) {
-    __shared__ int s_ref[kWfBlock / 32][kMaxStack];
-    __shared__ float s_key[kWfBlock / 32][kMaxStack];
+__global__ void __launch_bounds__(kWfMaxBlock) wf_extend_packet(WfArgs A) {
+    __shared__ int s_ref[kWfMaxBlock / 32][kMaxStack];
+    __shared__ float s_key[kWfMaxBlock / 32][kMaxStack];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int* sref = s_ref[warp];
     float* skey = s_key[warp];
@@ -503,10 +507,10 @@ struct StoreNee {
     }
 };
 
-// At most 72 registers (7 blocks per SM): the shading state machine is
+// At most 72 registers (28 warps per SM): the shading state machine is
 // latency-bound, and the extra resident warps pay for a few spilled words.
 template <bool COUNT, bool ONE>
-__global__ void __launch_bounds__(kWfBlock, 7)
+__global__ void __maxnreg__(72)
 wf_shade(WfArgs A, int it) {
     RayCount rc = {};
     QView qv = qview(A, it);
@@ -662,7 +666,7 @@ __global__ void __launch_bounds__(kSortChunk) wf_sort_chunks(int* chunk_off) {
 // Places every listed slot at its bin's next position (the order inside a
 // bin is arbitrary; a path's result does not depend on its queue position).
 // list[0, *count) -> out by keyof[e], the key stored beside list entry e.
-__global__ void __launch_bounds__(kWfBlock)
+__global__ void __launch_bounds__(kWfMaxBlock)
 wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
                 const int* chunk_off, int* out) {
     const int ns = *count;
@@ -690,7 +694,7 @@ wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
 // in the order shade made them, feeding each visibility into the same
 // NeeAccum as the megakernel, then applies the pending terms to L.
 template <bool COUNT, bool ONE>
-__global__ void __launch_bounds__(kWfBlock)
+__global__ void __launch_bounds__(kWfMaxBlock)
 wf_shadow(WfArgs A, int it) {
     extern __shared__ int smem[];
     TravStack<kWfShared> stk;
@@ -844,7 +848,7 @@ __device__ __forceinline__ void accumulate_pixel(const WfArgs& A, long long pix,
 }
 
 // A warp per pixel of the chunk, grid-stride over the pixels.
-__global__ void __launch_bounds__(kWfBlock)
+__global__ void __launch_bounds__(kWfMaxBlock)
 wf_accumulate(WfArgs A, long long pix_begin, int n_pix, long long path_begin) {
     const int g = threadIdx.x & 31;
     const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -854,8 +858,8 @@ wf_accumulate(WfArgs A, long long pix_begin, int n_pix, long long path_begin) {
 }
 
 // Blocks of wf_accumulate for `pixels` pixels: a warp each, at most `cap`.
-static unsigned accumulate_blocks(long long pixels, int cap) {
-    const long long b = (pixels * 32 + kWfBlock - 1) / kWfBlock;
+static unsigned accumulate_blocks(long long pixels, int cap, int block = kWfBlock) {
+    const long long b = (pixels * 32 + block - 1) / block;
     return (unsigned)(b < cap ? b : cap);
 }
 
@@ -882,6 +886,7 @@ struct WfScratch {
     int iters = 0;
     int jobs_cap = 0;
     int views_cap = 0;
+    int block = kWfBlock;             // threads per block of this frame's kernels
     WfArgs args{};
     SceneView* d_views = nullptr;
     WfJob* d_jobs = nullptr;
@@ -991,23 +996,23 @@ struct WfOccupancy {
 };
 
 template <bool COUNT, bool ONE>
-static cudaError_t occupancy(WfOccupancy& o) {
+static cudaError_t occupancy(WfOccupancy& o, int blk = kWfBlock) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    size_t smem = (size_t)kWfShared * kWfBlock * 8;
+    size_t smem = (size_t)kWfShared * blk * 8;
     int b1 = 0, b2 = 0, b3 = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, wf_extend<COUNT, ONE>, kWfBlock, smem);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, wf_shade<COUNT, ONE>, kWfBlock, 0);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, wf_shadow<COUNT, ONE>, kWfBlock, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, wf_extend<COUNT, ONE>, blk, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, wf_shade<COUNT, ONE>, blk, 0);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, wf_shadow<COUNT, ONE>, blk, smem);
     o.grid_extend = sms * std::max(b1, 1);
     o.grid_shade = sms * std::max(b2, 1);
     o.grid_shadow = sms * std::max(b3, 1);
     o.grid_scatter = sms * 8;
-    o.grid_accumulate = sms * 16;
+    o.grid_accumulate = sms * 16 * kWfBlock / blk;
     int b4 = 0;
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, wf_extend_packet<COUNT>, kWfBlock, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, wf_extend_packet<COUNT>, blk, 0);
     o.grid_packet = sms * std::max(b4, 1);
     return e;
 }
@@ -1044,8 +1049,9 @@ struct LaunchTimer {
 template <bool COUNT, bool ONE>
 static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& jobs, int iters,
                                  int Qeff, cudaStream_t st, int* launches, LaunchTimer& lt) {
+    const int blk = W.block;
     WfOccupancy occ;
-    cudaError_t e = occupancy<COUNT, ONE>(occ);
+    cudaError_t e = occupancy<COUNT, ONE>(occ, blk);
     if (e != cudaSuccess) return e;
     const bool packet_first = ONE && W.args.packets != 0;
     // timed (profiled) frames stay on one stream so that kernel classes add
@@ -1053,7 +1059,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
     // cross-stream waits would cost
     const bool overlap = W.side != nullptr && !lt.on && Qeff >= (1 << 20);
     const WfArgs& A = W.args;
-    const size_t smem = (size_t)kWfShared * kWfBlock * 8;
+    const size_t smem = (size_t)kWfShared * blk * 8;
     // walk the path space in chunks of whole pixels
     int ji = 0;
     long long pix_in_job = 0;
@@ -1081,9 +1087,9 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         if (A.sort_key >= 2 &&
             (e = cudaMemsetAsync(A.tcnt, 0, (size_t)(iters + 2) * 2 * 4, st)) != cudaSuccess)
             return e;
-        int gblocks = (int)((slots + kWfBlock - 1) / kWfBlock);
+        int gblocks = (int)((slots + blk - 1) / blk);
         lt.mark(KC_GENERATE, st, true);
-        wf_generate<COUNT, ONE><<<gblocks, kWfBlock, 0, st>>>(A, path_begin, (int)slots);
+        wf_generate<COUNT, ONE><<<gblocks, blk, 0, st>>>(A, path_begin, (int)slots);
         lt.mark(KC_GENERATE, st, false);
         n_launch += 1;
         // With a side stream, shadow k runs on it beside extend k+1 (they
@@ -1093,9 +1099,9 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         auto launch_extend = [&](int it) {
             lt.mark(KC_EXTEND, st, true);
             if (it == 0 && packet_first)
-                wf_extend_packet<COUNT><<<occ.grid_packet, kWfBlock, 0, st>>>(A);
+                wf_extend_packet<COUNT><<<occ.grid_packet, blk, 0, st>>>(A);
             else
-                wf_extend<COUNT, ONE><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
+                wf_extend<COUNT, ONE><<<occ.grid_extend, blk, smem, st>>>(A, it);
             lt.mark(KC_EXTEND, st, false);
         };
         if (iters > 0) launch_extend(0);
@@ -1111,7 +1117,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
             if (sort_next &&
                 (e = cudaMemsetAsync(A.hist_e, 0, (size_t)kSortBinsE * 4, st)) != cudaSuccess)
                 return e;
-            wf_shade<COUNT, ONE><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
+            wf_shade<COUNT, ONE><<<occ.grid_shade, blk, 0, st>>>(A, it);
             if (A.sort_key >= 2) {
                 wf_sort_scan<<<kSortChunks, kSortChunk, 0, st>>>(A.hist_s, A.chunk_off);
                 wf_sort_chunks<kSortChunks><<<1, kSortChunk, 0, st>>>(A.chunk_off);
@@ -1132,12 +1138,12 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
             if (overlap) {
                 if ((e = cudaEventRecord(W.ev_shaded, st)) != cudaSuccess) return e;
                 if ((e = cudaStreamWaitEvent(W.side, W.ev_shaded, 0)) != cudaSuccess) return e;
-                wf_shadow<COUNT, ONE><<<occ.grid_shadow, kWfBlock, smem, W.side>>>(A, it);
+                wf_shadow<COUNT, ONE><<<occ.grid_shadow, blk, smem, W.side>>>(A, it);
                 if ((e = cudaEventRecord(W.ev_shadow, W.side)) != cudaSuccess) return e;
                 if (it + 1 < iters) launch_extend(it + 1);
             } else {
                 lt.mark(KC_SHADOW, st, true);
-                wf_shadow<COUNT, ONE><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
+                wf_shadow<COUNT, ONE><<<occ.grid_shadow, blk, smem, st>>>(A, it);
                 lt.mark(KC_SHADOW, st, false);
                 if (it + 1 < iters) launch_extend(it + 1);
             }
@@ -1145,9 +1151,9 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         }
         if (overlap && iters > 0 && (e = cudaStreamWaitEvent(st, W.ev_shadow, 0)) != cudaSuccess)
             return e;
-        const unsigned ablocks = accumulate_blocks(pixels, occ.grid_accumulate);
+        const unsigned ablocks = accumulate_blocks(pixels, occ.grid_accumulate, blk);
         lt.mark(KC_ACCUMULATE, st, true);
-        wf_accumulate<<<ablocks, kWfBlock, 0, st>>>(A, pix_begin, (int)pixels, path_begin);
+        wf_accumulate<<<ablocks, blk, 0, st>>>(A, pix_begin, (int)pixels, path_begin);
         lt.mark(KC_ACCUMULATE, st, false);
         n_launch += 1;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1170,7 +1176,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     int iters = 0, maxS = 1, max_spp = 1;
     long long total_paths = 0;
     bool count = false;
-    int qcap = 0, sort_key = 0, refill = 0;
+    int qcap = 0, sort_key = 0, refill = 0, block = 0;
     bool packets = true;
     for (int k = 0; k < n; ++k) {
         const RenderCfg& c = cfgs[k];
@@ -1192,6 +1198,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
         if (c.queue_capacity > 0) qcap = c.queue_capacity;
         sort_key = c.sort_key;
         if (c.refill > 0) refill = c.refill;
+        if (c.block > 0) block = c.block;
         packets = packets && c.packets;
     }
     total_paths = path_off;
@@ -1207,6 +1214,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     W.args.packets = packets ? 1 : 0;
     W.args.refill_below = refill > 0 ? refill : kDefaultRefill;
     W.args.maxS = maxS;
+    W.block = block > 0 ? block : kWfBlock;
     const bool one = n == 1;
     if (one) {
         W.args.view0 = views[jobs[0].view];
@@ -1234,6 +1242,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     mix((unsigned long long)sort_key);
     mix((unsigned long long)W.args.packets);
     mix((unsigned long long)W.args.refill_below);
+    mix((unsigned long long)W.block);
     mix((unsigned long long)count);
     for (const auto& J : jobs) {
         mix((unsigned long long)J.P.W); mix((unsigned long long)J.P.H);
@@ -1376,7 +1385,9 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 size_t static_scratch_bytes() { return kStaticBytes; }
 
 // Device address of g_static_scratch on the current device, looked up once
-// per device (cudaGetSymbolAddress) and cached.
+// per device (cudaGetSymbolAddress) and cached for the life of the process.
+// The cache assumes the device's primary context lives as long as the
+// library: after a cudaDeviceReset the cached address would be stale.
 static std::mutex g_static_mu;
 static void* g_static_ptr[64];
 
@@ -1420,7 +1431,12 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
         *why = "depth above 64 is beyond the no-allocation render";
         return cudaErrorInvalidValue;
     }
-    if (c.spp > kStaticSlots || c.sort_key != 0 || c.count || c.profile) {
+    if (c.spp > kStaticSlots) {
+        *why = "more than 65536 samples per pixel do not fit the no-allocation render's "
+               "paths in flight";
+        return cudaErrorInvalidValue;
+    }
+    if (c.sort_key != 0 || c.count || c.profile) {
         *why = "the no-allocation render takes no ray sorting, counting or profiling";
         return cudaErrorInvalidValue;
     }

@@ -48,6 +48,8 @@ class RenderSettings:
     queue_capacity: int = 0
     sort_key: int = 0
     refill_below: int = 0
+    block_size: int = 0            # wavefront threads per block (0: 128)
+    binary_tree: bool = False      # megakernel on Pencil's binary tree
 
     def params(self) -> A.RenderParams:
         p = A.RenderParams()
@@ -64,9 +66,11 @@ class RenderSettings:
                    (0 if self.use_graph else A.FLAG_NO_GRAPH) |
                    (A.FLAG_PROFILE_KERNELS if self.profile_kernels else 0) |
                    (0 if self.packets else A.FLAG_NO_PACKETS) |
-                   (A.FLAG_MIS if self.mis else 0))
+                   (A.FLAG_MIS if self.mis else 0) |
+                   (A.FLAG_BINARY_TREE if self.binary_tree else 0))
         p.queue_capacity, p.sort_key = self.queue_capacity, self.sort_key
         p.refill_below = self.refill_below
+        p.block_size = self.block_size
         return p
 
 

@@ -1,9 +1,10 @@
 """Generate the golden fixtures of tests/golden from the reference renderer.
 
 Run in a checkout next to the reference project (its sources and its own
-golden PNGs); needs oracle/_ref/pencil_ref, built by `make -C oracle`:
+golden PNGs); needs oracle/_ref/pencil_ref, built by
+`make -C oracle REF_SRC=/path/to/pencil/src`:
 
-    python tests/golden/make_golden.py [--ref /path/to/pencil]
+    python tests/golden/make_golden.py --ref /path/to/pencil
 
 Writes, for each fixture scene:
   scenes/<name>.bin   the scene (PGPUSCN1 format): the reference's parser output
@@ -16,7 +17,10 @@ Writes, for each fixture scene:
 and png_goldens.json: digests of the reference's own golden PNGs
 (tests/three_spheres.png, tests/shapes.png: SHA-256 of the decoded RGB;
 tests/cornell_box.png: a seeded sample of pixels, since the current code
-reproduces it to within 1 LSB only).
+reproduces it to within 1 LSB only), and config_pins.json: SHA-256 digests
+of the reference renderer's HDR output (and BVH) on the benchmark
+configurations' own scenes at their configured image sizes (`--only configs`
+writes just this file).
 """
 from __future__ import annotations
 
@@ -118,6 +122,41 @@ def fixture(name: str, scene: Scene, wh: tuple[int, int, int, int], rng) -> dict
     return d
 
 
+def _sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def config_pins() -> dict:
+    """Reference renders of the benchmark configurations' scenes.
+
+    c1_pt / c1_wh  three spheres, 320x240, n=2, depth 8 (path tracer / Whitted)
+    c2_n1          the 100k-sphere cloud at its full 1280x720 frame, depth 8,
+                   n=1 (the configured n=4 costs the reference 16x longer; the
+                   sample loop, jitter and seeding are the same code at any n)
+    c3_128         the full 1,310,720-triangle mesh box (the reference reaches
+                   its emitter by BSDF sampling only), 128x128, n=1, depth 12
+    c5_pt          the adjoint box (1,000 spheres), 512x512, n=4, depth 6
+    Each entry: the settings, the SHA-256 of the HDR floats, their mean, the
+    trace-call count and the SHA-256 of the reference's BVH node table."""
+    cases = {
+        "c1_pt": (W.three_spheres_pt(320, 240, 2, 8).scene, (320, 240, 2, 8), True),
+        "c1_wh": (W.three_spheres_pt(320, 240, 2, 8).scene, (320, 240, 2, 8), False),
+        "c2_n1": (W.sphere_cloud().scene, (1280, 720, 1, 8), True),
+        "c3_128": (no_quad_lights(W.mesh_box().scene), (128, 128, 1, 12), True),
+        "c5_pt": (no_quad_lights(W.adjoint_box()[0].scene), (512, 512, 4, 6), True),
+    }
+    out = {}
+    for name, (scene, (w, h, n, depth), pt) in cases.items():
+        _, nodes, tdepth = O.ref_dump(scene)
+        img, info = O.ref_render(scene, w, h, n, depth, pt, threads=8)
+        out[name] = {"settings": [w, h, n, depth], "pathtrace": pt, "hdr_sha256": _sha(img),
+                     "hdr_mean": float(img.astype(np.float64).mean()),
+                     "rays": int(info["rays"]), "nodes_sha256": _sha(nodes),
+                     "bvh_depth": int(tdepth)}
+        print("pinned", name, out[name]["hdr_mean"])
+    return out
+
+
 def png_goldens(ref_root: Path) -> dict:
     from PIL import Image
     rng = np.random.default_rng(11)
@@ -137,11 +176,18 @@ def png_goldens(ref_root: Path) -> dict:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True,
+                    help="root of the reference project (holds src/, examples/, tests/)")
+    ap.add_argument("--only", choices=["configs"], default=None,
+                    help="write only config_pins.json")
     a = ap.parse_args()
     ref_root = Path(a.ref)
     if not O.ref_available():
         raise SystemExit("oracle/_ref/pencil_ref is missing: run `make -C oracle` first")
+    if a.only == "configs":
+        (HERE / "config_pins.json").write_text(json.dumps(config_pins(), indent=1))
+        print("wrote config_pins.json")
+        return
     (HERE / "scenes").mkdir(exist_ok=True)
     rng = np.random.default_rng(1234)
     scenes = {}
@@ -162,6 +208,8 @@ def main() -> None:
         gold[name]["render"] = meta[name]
     (HERE / "png_goldens.json").write_text(json.dumps(gold))
     print("wrote png_goldens.json")
+    (HERE / "config_pins.json").write_text(json.dumps(config_pins(), indent=1))
+    print("wrote config_pins.json")
 
 
 if __name__ == "__main__":

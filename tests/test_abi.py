@@ -32,9 +32,9 @@ def test_library_exports_every_declared_function():
 
 def test_abi_version_and_record_sizes():
     lib = A.load()
-    assert lib.pgpu_abi_version() == 1
+    assert lib.pgpu_abi_version() == A.ABI_VERSION == 2
     assert C.sizeof(A.Camera) == 52
-    assert C.sizeof(A.RenderParams) == 64
+    assert C.sizeof(A.RenderParams) == 68
     assert C.sizeof(A.Stats) == 152
     assert C.sizeof(A.SceneInfo) == 32
 

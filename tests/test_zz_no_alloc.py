@@ -66,6 +66,35 @@ def test_noalloc_equals_render_on_two_calls_in_a_row(gpu, name, pathtrace):
     gpu.free(sid)
 
 
+@pytest.mark.parametrize("name,samples", [("cornell_box", 3), ("cloud2k", 2)])
+def test_noalloc_several_chunks_equal_render(gpu, name, samples):
+    """More paths than the 65,536 the array holds at once, so the render runs
+    chunk after chunk and the last chunk is partial: 128x96 pixels at 9
+    samples are 110,592 paths (chunks of 7,281 and 5,007 pixels); 192x128 at
+    4 samples are 98,304 paths (16,384 and 8,192 pixels). Each chunk must
+    restart its queues and cursors and accumulate into its own pixels; the
+    image equals pgpu_render's bit for bit, twice in a row."""
+    scene, nodes, st = case(name)
+    st.width, st.height, st.samples = 128, 96, samples
+    if samples == 2:
+        st.width, st.height = 192, 128
+    assert st.width * st.height * samples * samples > 65536
+    sid = gpu.upload(scene, nodes)
+    ref = gpu.render(sid, st)
+    m2_ref = np.zeros_like(ref)
+    gpu.render(sid, st, m2=m2_ref)
+    out = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")
+    m2 = torch.empty_like(out)
+    for _ in range(2):
+        out.fill_(float("nan"))
+        m2.fill_(float("nan"))
+        torch.cuda.synchronize()
+        gpu.check(noalloc(gpu, sid, st, out, m2), "pgpu_render_noalloc")
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+        assert np.array_equal(m2.cpu().numpy().view(np.uint32), m2_ref.view(np.uint32))
+    gpu.free(sid)
+
+
 def test_noalloc_allocates_nothing(gpu):
     scene, nodes, st = case("cloud2k")
     sid = gpu.upload(scene, nodes)
