@@ -27,6 +27,7 @@ the same workload on this host's cores.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import re
@@ -46,7 +47,14 @@ sys.path.insert(0, str(ROOT))
 METRIC = ("Mpaths/s & Mrays/s at equal RMSE, wavefront vs megakernel (1 B200); "
           "adjoint ms/grad")
 WORKLOAD = "sphere_cloud_100k_1280x720_n4_16spp_depth8"
-CPU_SAMPLE = (320, 180, 4, 8)      # width, height, n, depth of the bounded CPU sample
+# The bounded CPU sample: the full frame at n=2 (4 spp instead of 16; the
+# per-path work is the same), 240 of Pencil's 64x64 tiles, so every host
+# thread gets many tiles and none idles at the end.
+CPU_SAMPLE = (1280, 720, 2, 8)     # width, height, n, depth
+CPU_RUNS = 3                       # timed runs (median) after one warm-up run
+# Window of the frame whose paths the oracle replays to count the
+# reference-order traversal work (algorithmic bytes).
+COUNT_WINDOW = (480, 270, 320, 180)
 
 
 def parse_args():
@@ -143,9 +151,34 @@ def cpu_reference_run(scene, steps: int, warmup: int) -> dict:
         kind = "port"
     med = statistics.median(secs)
     return {"value": paths / med / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": kind,
-            "sample": f"the same 100k-sphere scene at {w}x{h}, n={n} ({n*n} spp), depth {depth}: "
-                      f"{paths} paths per run, median of {len(secs)} runs",
+            "sample": f"the same 100k-sphere frame at {w}x{h}, n={n} ({n*n} spp), depth {depth}: "
+                      f"{paths} paths and {-(-w // 64) * -(-h // 64)} 64x64 tiles per run, "
+                      f"median of {len(secs)} runs after {warmup} warm-up",
             "seconds": secs}
+
+
+def reference_order_counts(scene, settings) -> dict:
+    """Algorithmic work per ray of the frame's paths, counted by the oracle
+    on COUNT_WINDOW: its replay of the production estimator walks Pencil's
+    binary tree in Pencil's own order (BVHNode::hit / occluded: left child,
+    then right, every box tested), so the node and primitive counts are the
+    reference algorithm's for the very rays the GPU traces."""
+    import dataclasses
+
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    _, _, cnt = O.Oracle(scene).render_split(dataclasses.replace(settings),
+                                             window=COUNT_WINDOW)
+    ext, sh = int(cnt[O.CNT_EXTENSION_RAYS]), int(cnt[O.CNT_SHADOW_RAYS])
+    x, y, w, h = COUNT_WINDOW
+    paths = w * h * settings.samples ** 2
+    return {"window": list(COUNT_WINDOW), "paths": paths,
+            "ext_rays_per_path": ext / paths, "shadow_rays_per_path": sh / paths,
+            "ext_nodes_per_ray": float(cnt[O.CNT_EXT_NODES]) / max(ext, 1),
+            "ext_prim_bytes_per_ray": float(cnt[O.CNT_EXT_PRIM_BYTES]) / max(ext, 1),
+            "shadow_nodes_per_ray": float(cnt[O.CNT_SH_NODES]) / max(sh, 1),
+            "shadow_prim_bytes_per_ray": float(cnt[O.CNT_SH_PRIM_BYTES]) / max(sh, 1),
+            "seconds": time.perf_counter() - t0}
 
 
 def run_reference(args) -> None:
@@ -156,8 +189,8 @@ def run_reference(args) -> None:
     wl = W.sphere_cloud()
     steps, warmup = max(args.steps, 1), max(args.warmup, 0)
     # each step is one bounded-sample render; keep the whole run to a few minutes
-    steps = min(steps, 10)
-    warmup = min(warmup, 3)
+    steps = min(steps, 8)
+    warmup = min(warmup, 1)
     cb = cpu_reference_run(wl.scene, steps, warmup)
     ms = statistics.median(cb["seconds"]) * 1e3
     line = {"metric": METRIC, "value": cb["value"], "unit": "Mpaths/s", "n_gpus": args.gpus,
@@ -180,14 +213,21 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def ncu_traffic_per_ray() -> float | None:
-    """DRAM bytes per extension ray of wf_extend, from the committed ncu
-    summary (profiles/wf_extend_sphere_cloud.txt), if present."""
+def ncu_per_ray() -> dict:
+    """Per-extension-ray DRAM bytes, L2 sectors and L2 throughput of one
+    wf_extend launch, from the committed ncu summary
+    (profiles/wf_extend_sphere_cloud.txt), where present."""
     p = ROOT / "profiles" / "wf_extend_sphere_cloud.txt"
+    out = {}
     if not p.exists():
-        return None
-    m = re.search(r"dram_bytes_per_ray:\s*([0-9.eE+-]+)", p.read_text())
-    return float(m.group(1)) if m else None
+        return out
+    text = p.read_text()
+    for key in ("dram_bytes_per_ray", "l2_sectors_per_ray", "l2_throughput_pct",
+                "dram_throughput_pct"):
+        m = re.search(key + r":\s*([0-9.eE+-]+)", text)
+        if m:
+            out[key] = float(m.group(1))
+    return out
 
 
 def run_ours(args) -> None:
@@ -262,7 +302,12 @@ def run_ours(args) -> None:
     ms_wf = timed(A.ENGINE_WAVEFRONT, args.steps, args.warmup, clocks)
     clk = clocks.summary()
     mk_steps = max(2, min(args.steps, 5))
+    # the plain megakernel on the same 4-wide tree (the baseline), and on
+    # Pencil's binary tree
     ms_mk = timed(A.ENGINE_MEGAKERNEL, mk_steps, 1)
+    st.binary_tree = True
+    ms_mk_bin = timed(A.ENGINE_MEGAKERNEL, mk_steps, 1)
+    st.binary_tree = False
     value = paths_per_frame * world / (ms_wf * 1e-3) / 1e6
     mk_value = paths_per_frame * world / (ms_mk * 1e-3) / 1e6
 
@@ -280,31 +325,70 @@ def run_ours(args) -> None:
     rays = cnt.extension_rays + cnt.shadow_rays
     mrays = rays * world / (ms_wf * 1e-3) / 1e6
 
-    # roofline of the dominant kernel (closest-hit traversal, wf_extend)
+    # roofline of the dominant kernel (closest-hit traversal, wf_extend):
+    # algorithmic bytes of the reference algorithm per extension ray -- 32 B
+    # per binary node Pencil's walk visits, the primitive records it tests,
+    # and the queue traffic of one ray (origin + direction read, hit record
+    # written, queue slot read: 52 B) -- counted by the oracle on rank 0
     kms = prof.kernel_ms
     dominant = max(("extend", "shade", "shadow", "generate", "accumulate"), key=lambda k: kms[k])
-    # extend launches per frame: one per bounce and chunk of queue_capacity paths
     chunk = st.queue_capacity if st.queue_capacity > 0 else paths_per_frame
-    ext_launches = -(-paths_per_frame // max(1, chunk)) * st.pathtrace_bounces
-    per_ray_queue = 16 + 16 + 16 + 4 + 16            # ray o, d, state, queue slot; hit write
-    wide_node_bytes = 7 * 16                         # 4-wide node: 6 planes x 4 boxes + refs
-    alg_bytes = (cnt.ext_node_visits * wide_node_bytes + cnt.ext_leaf_bytes +
-                 cnt.extension_rays * per_ray_queue)
-    n_ext_launches = max(1, ext_launches)
-    achieved = alg_bytes / (kms["extend"] * 1e-3) / 1e9
+    n_ext_launches = max(1, -(-paths_per_frame // max(1, chunk)) * st.pathtrace_bounces)
+    ext_launch_ms = kms["extend"] / n_ext_launches
+    rays_per_launch = cnt.extension_rays / n_ext_launches
     peaks = measured_peaks()
-    tr = ncu_traffic_per_ray()
-    roof = {"kernel": "wf_extend", "bound": "hbm", "achieved": achieved,
-            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-            "traffic": (tr * cnt.extension_rays / n_ext_launches) if tr else None,
-            "algorithmic_bytes_per_launch": alg_bytes / n_ext_launches,
-            "launches": n_ext_launches,
-            "avg_launch_ms": kms["extend"] / n_ext_launches,
-            "peak_source": peaks["source"],
-            "bytes_per_ray": alg_bytes / max(1, cnt.extension_rays),
-            "nodes_per_ray": cnt.ext_node_visits / max(1, cnt.extension_rays),
-            "dominant_kernel_by_time": dominant,
-            "kernel_ms": kms}
+    ncu = ncu_per_ray()
+    ref_counts = None
+    if rank == 0:
+        try:
+            ref_counts = reference_order_counts(wl.scene, dataclasses.replace(st))
+        except Exception as ex:  # noqa: BLE001
+            ref_counts = {"error": str(ex)}
+    roof = {"kernel": "wf_extend", "bound": "hbm", "unit": "GB/s", "peak": peaks["hbm_gbs"],
+            "peak_source": peaks["source"], "launches": n_ext_launches,
+            "avg_launch_ms": ext_launch_ms, "rays_per_launch": rays_per_launch,
+            "dominant_kernel_by_time": dominant, "kernel_ms": kms,
+            "gpu_wide_nodes_per_ray": cnt.ext_node_visits / max(1, cnt.extension_rays)}
+    if ref_counts and "ext_nodes_per_ray" in ref_counts:
+        per_ray = (32.0 * ref_counts["ext_nodes_per_ray"] + ref_counts["ext_prim_bytes_per_ray"]
+                   + 52.0)
+        alg = per_ray * rays_per_launch
+        achieved = alg / (ext_launch_ms * 1e-3) / 1e9
+        roof.update({"achieved": achieved, "frac": achieved / peaks["hbm_gbs"],
+                     "algorithmic_bytes_per_launch": alg,
+                     "algorithmic_bytes_per_ray": per_ray,
+                     "reference_order": ref_counts})
+    else:
+        roof.update({"achieved": None, "frac": None, "reference_order": ref_counts})
+    # what the memory system actually carried (ncu, one launch, scaled per ray)
+    roof["traffic"] = (ncu["dram_bytes_per_ray"] * rays_per_launch
+                       if "dram_bytes_per_ray" in ncu else None)
+    if roof["traffic"] is not None:
+        dram_gbs = roof["traffic"] / (ext_launch_ms * 1e-3) / 1e9
+        roof["dram_achieved_gbs"] = dram_gbs
+        roof["dram_frac"] = dram_gbs / peaks["hbm_gbs"]
+    if "l2_sectors_per_ray" in ncu:
+        l2_bytes = 32.0 * ncu["l2_sectors_per_ray"] * rays_per_launch
+        roof["l2_bytes_per_launch"] = l2_bytes
+        roof["l2_achieved_gbs"] = l2_bytes / (ext_launch_ms * 1e-3) / 1e9
+    if "l2_throughput_pct" in ncu:
+        roof["l2_frac"] = ncu["l2_throughput_pct"] / 100.0
+    roof["limiter"] = ("latency of L1/L2-resident node loads (the 23 MB scene arena stays in "
+                       "the 126 MB L2): DRAM and L2 fractions from ncu below 1, long-scoreboard "
+                       "stalls; frac above 1 means the kernel finishes the reference "
+                       "algorithm's node traffic faster than HBM could stream it")
+    # the frame as a whole, per the same definition: bytes per path of every
+    # segment (node/primitive bytes + ray, hit and path state read and
+    # written, 192 B) and every shadow ray
+    if ref_counts and "ext_nodes_per_ray" in ref_counts:
+        per_path = (ref_counts["ext_rays_per_path"] *
+                    (32.0 * ref_counts["ext_nodes_per_ray"] + ref_counts["ext_prim_bytes_per_ray"]
+                     + 192.0) +
+                    ref_counts["shadow_rays_per_path"] *
+                    (32.0 * ref_counts["shadow_nodes_per_ray"] +
+                     ref_counts["shadow_prim_bytes_per_ray"] + 48.0))
+        roof["frame"] = {"bytes_per_path": per_path,
+                         "achieved_gbs": per_path * value * 1e6 / 1e9 / world}
 
     # e2e through the C-ABI with host buffers
     e2e = None
@@ -348,7 +432,7 @@ def run_ours(args) -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_reference_run(wl.scene, 1, 0)
+            cb = cpu_reference_run(wl.scene, CPU_RUNS, 1)
             cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as ex:  # noqa: BLE001
             cpu = {"value": None, "unit": "Mpaths/s", "cores": os.cpu_count(), "kind": "reference",
@@ -371,7 +455,11 @@ def run_ours(args) -> None:
                                       else "1 GPU"},
             "mrays_per_s": mrays,
             "rays_per_step": rays,
-            "megakernel": {"value": mk_value, "unit": "Mpaths/s", "ms_per_step": ms_mk},
+            "megakernel": {"value": mk_value, "unit": "Mpaths/s", "ms_per_step": ms_mk,
+                           "tree": "4-wide (the tree the wavefront walks)"},
+            "megakernel_binary_tree": {"value": paths_per_frame * world / (ms_mk_bin * 1e-3) / 1e6,
+                                       "unit": "Mpaths/s", "ms_per_step": ms_mk_bin,
+                                       "tree": "Pencil's binary tree"},
             "wavefront_over_megakernel": ms_mk / ms_wf,
             "equal_rmse": "bit-identical images (same estimator, same random numbers)",
             "roofline": roof,
@@ -413,25 +501,7 @@ def measure_extras(ctx, sid, st, img, stream) -> dict:
     import torch
     from pencil_b200 import _abi as A
     from pencil_b200 import workloads as W
-    out = {}
-    # quality: relative RMSE of the 16-spp frame against 4096 spp (256 frames
-    # of 16 spp with distinct sample offsets, averaged on the device)
-    ref = torch.zeros_like(img)
-    q = dataclasses.replace(st, engine=A.ENGINE_WAVEFRONT)
-    frames = 256
-    for k in range(frames):
-        q.sample_offset = (k + 1000) * st.samples * st.samples
-        ctx.render_device(sid, q, img.data_ptr())
-        ref += img
-    ref /= frames
-    q.sample_offset = 0
-    ctx.render_device(sid, q, img.data_ptr())
-    rel_rmse = float(torch.sqrt(((img - ref) ** 2).mean()) / ref.mean())
-    spp = st.samples ** 2
-    out["quality"] = {"rel_rmse_vs_4096spp": rel_rmse, "spp": spp,
-                      "spp_for_1pct_rmse": int(np.ceil(spp * (rel_rmse / 0.01) ** 2)),
-                      "note": "wavefront and megakernel images are bit-identical, so their RMSE "
-                              "is equal at every spp"}
+    out = {"quality": measure_quality(ctx, sid, st, stream)}
     # adjoint of the box configuration: 1,000 spheres, 512x512, 16 spp, depth 6
     wa, _, _ = W.adjoint_box()
     sa = ctx.upload(wa.scene)
@@ -459,7 +529,12 @@ def measure_extras(ctx, sid, st, img, stream) -> dict:
     ptrs = [o.data_ptr() for o in outs]
     paths = sum(x.width * x.height * x.samples ** 2 for x in sts)
     for x in sts:
-        x.queue_capacity, x.refill_below = 1 << 24, 16
+        x.queue_capacity, x.refill_below, x.sort_key, x.block_size = 1 << 24, 16, 0, 0
+    fixed_ms = _event_ms(stream, lambda: ctx.render_batch(sids, sts, device_ptrs=ptrs), 2)
+    # the batch's launch parameters from the autotuner (capacity, refill,
+    # sort key, block size), timed once each
+    from pencil_b200.autotune import autotune
+    tuned = autotune(ctx, sids, sts, reps=1, use_cache=False)
     batch_ms = _event_ms(stream, lambda: ctx.render_batch(sids, sts, device_ptrs=ptrs), 2)
 
     def one_by_one(engine):
@@ -473,14 +548,133 @@ def measure_extras(ctx, sid, st, img, stream) -> dict:
     out["batch"] = {"workload": "256 random-sphere scenes, 10-50,000 spheres, 128/256/512 "
                                 "squared, 1/4/16/64 spp, depth 8",
                     "paths": paths, "batched_mpaths_s": paths / batch_ms / 1e3,
+                    "batched_fixed_mpaths_s": paths / fixed_ms / 1e3,
+                    "fixed_params": {"queue_capacity": 1 << 24, "refill_below": 16,
+                                     "sort_key": 0, "block_size": 128},
+                    "autotuned": {k: tuned[k] for k in ("queue_capacity", "refill_below",
+                                                         "sort_key", "block_size")},
                     "one_by_one_wavefront_mpaths_s": paths / seq_ms / 1e3,
                     "one_by_one_megakernel_mpaths_s": paths / mk_ms / 1e3,
-                    "batched_ms": batch_ms, "one_by_one_wavefront_ms": seq_ms,
+                    "batched_ms": batch_ms, "batched_fixed_ms": fixed_ms,
+                    "one_by_one_wavefront_ms": seq_ms,
                     "one_by_one_megakernel_ms": mk_ms}
     for s_ in sids:
         ctx.free(s_)
     out["mesh"] = measure_mesh(ctx, stream)
     out["bvh_build"] = measure_bvh_build(ctx, stream)
+    return out
+
+
+def _once_ms(stream, fn) -> float:
+    """Device ms of one call of a long render (CUDA events around it)."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _rel_rmse(img, ref) -> float:
+    import torch
+    return float(torch.sqrt(((img - ref) ** 2).mean()) / ref.mean())
+
+
+def _equal_rmse_point(ctx, sid, st, ref, stream, target=0.01) -> dict:
+    """The samples per pixel at which the production estimator's image is
+    within `target` relative RMSE of `ref`, and the time of both engines to
+    render the frame at that point. The RMSE model e^2 = a/spp + b (b: the
+    reference's own noise) is fitted from renders at n=4 and n=16."""
+    import torch
+    from pencil_b200 import _abi as A
+    img = torch.empty_like(ref)
+    q = dataclasses.replace(st, engine=A.ENGINE_WAVEFRONT)
+    e = {}
+    for n in (4, 16):
+        q.samples = n
+        ctx.render_device(sid, q, img.data_ptr())
+        e[n] = _rel_rmse(img, ref)
+    a = (e[4] ** 2 - e[16] ** 2) / (1 / 16 - 1 / 256)
+    b = max(e[4] ** 2 - a / 16, 0.0)
+    out = {"rel_rmse_16spp": e[4], "rel_rmse_256spp": e[16], "reference_noise_rel_rmse": b ** 0.5}
+    if b >= target ** 2 or a <= 0:
+        out["reachable"] = False
+        return out
+    n = min(64, int(np.ceil(np.sqrt(a / (target ** 2 - b)))))
+    res = {}
+    for name, eng in (("wavefront", A.ENGINE_WAVEFRONT), ("megakernel", A.ENGINE_MEGAKERNEL)):
+        q = dataclasses.replace(st, engine=eng, samples=n)
+        ms = _once_ms(stream, lambda: ctx.render_device(sid, q, img.data_ptr()))
+        paths = q.width * q.height * n * n
+        res[name] = {"ms": ms, "mpaths_s": paths / ms / 1e3, "rel_rmse": _rel_rmse(img, ref)}
+    out.update({"reachable": True, "spp": n * n, "n": n, **res,
+                "wavefront_over_megakernel": res["megakernel"]["ms"] / res["wavefront"]["ms"]})
+    return out
+
+
+def measure_quality(ctx, sid, st, stream) -> dict:
+    """Image quality at the north star's operating point (relative RMSE <=
+    1% against a 4096-spp reference).
+
+    Sphere cloud, the full frame: the reference image is the reference's
+    own estimator -- trace_path with both dielectric branches (the
+    megakernel's exact glass mode) -- at 4096 spp, rendered as 64 frames of
+    64 spp with distinct sample offsets. Mesh box (the displaced icosphere,
+    quad light): the frame at 256x256, reference 4096 spp of the production
+    estimator; the reference's own estimator (BSDF sampling only: the small
+    emitter is found by chance) is measured against it too."""
+    import torch
+    from pencil_b200 import _abi as A
+    from pencil_b200 import workloads as W
+    out = {}
+    ref = torch.zeros((st.height, st.width, 3), dtype=torch.float32, device="cuda")
+    img = torch.empty_like(ref)
+    q = dataclasses.replace(st, engine=A.ENGINE_MEGAKERNEL, glass=A.GLASS_BOTH_BRANCHES,
+                            samples=8)
+    frames = 64
+    t0 = time.perf_counter()
+    for k in range(frames):
+        q.sample_offset = (k + 1000) * 64
+        ctx.render_device(sid, q, img.data_ptr())
+        ref += img
+    ref /= frames
+    torch.cuda.synchronize()
+    out["sphere_cloud"] = {"reference": "trace_path with both glass branches, 4096 spp",
+                           "reference_seconds": time.perf_counter() - t0,
+                           **_equal_rmse_point(ctx, sid, st, ref, stream)}
+    # mesh box at 256x256
+    wm = W.mesh_box(width=256, height=256)
+    nodes, _ = wm.scene.build_bvh()
+    sm = ctx.upload(wm.scene, nodes)
+    sm_st = wm.settings
+    mref = torch.zeros((256, 256, 3), dtype=torch.float32, device="cuda")
+    mimg = torch.empty_like(mref)
+    q = dataclasses.replace(sm_st, engine=A.ENGINE_WAVEFRONT, samples=8)
+    for k in range(frames):
+        q.sample_offset = (k + 1000) * 64
+        ctx.render_device(sm, q, mimg.data_ptr())
+        mref += mimg
+    mref /= frames
+    rec = {"workload": "mesh_box at 256x256, depth 12",
+           "reference": "production estimator (quad-light NEE), 4096 spp",
+           **_equal_rmse_point(ctx, sm, sm_st, mref, stream)}
+    # the reference's own estimator (no quad light: BSDF sampling only) at
+    # 4096 spp against that image
+    bs = wm.scene
+    bs.lights = [l for l in bs.lights if l.kind != A.LIGHT_QUAD]
+    sb = ctx.upload(bs, nodes)
+    acc = torch.zeros_like(mref)
+    for k in range(frames):
+        q.sample_offset = (k + 1000) * 64
+        ctx.render_device(sb, q, mimg.data_ptr())
+        acc += mimg
+    acc /= frames
+    rec["bsdf_only_4096spp_rel_rmse"] = _rel_rmse(acc, mref)
+    ctx.free(sb)
+    ctx.free(sm)
+    out["mesh_box"] = rec
     return out
 
 
@@ -553,6 +747,9 @@ def measure_mesh(ctx, stream) -> dict:
     st.count_rays = False
     st.engine = A.ENGINE_MEGAKERNEL
     mk_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 1)
+    st.binary_tree = True
+    mk_bin_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 1)
+    st.binary_tree = False
     ctx.free(sm)
     rays = cnt.extension_rays + cnt.shadow_rays
     return {"workload": "mesh_box: displaced icosphere 1,310,720 triangles in a box, quad-light "
@@ -563,9 +760,10 @@ def measure_mesh(ctx, stream) -> dict:
             "wavefront_ms": wf_ms, "wavefront_mpaths_s": paths / wf_ms / 1e3,
             "wavefront_mrays_s": rays / wf_ms / 1e3,
             "megakernel_ms": mk_ms, "megakernel_mpaths_s": paths / mk_ms / 1e3,
+            "megakernel_binary_tree_ms": mk_bin_ms,
             "wavefront_over_megakernel": mk_ms / wf_ms,
             "autotuned": {k: tuned[k] for k in ("queue_capacity", "refill_below", "sort_key",
-                                                 "ms")}}
+                                                 "block_size", "ms")}}
 
 
 class _Null:

@@ -47,11 +47,11 @@ enum pgpu_status {
     PGPU_ERR_UNSUPPORTED     = -2,  /* scene feature outside the GPU core    */
     PGPU_ERR_CUDA            = -3,  /* a CUDA runtime call failed            */
     PGPU_ERR_QUEUE_OVERFLOW  = -4,  /* a device queue ran out of capacity    */
-    PGPU_ERR_TIMEOUT         = -5,  /* device work exceeded its time budget  */
+    PGPU_ERR_TIMEOUT         = -5,  /* device work exceeded the time budget
+                                       of pgpu_set_timeout                   */
     PGPU_ERR_NO_SCENE        = -6,  /* unknown or freed scene id             */
     PGPU_ERR_OUT_OF_MEMORY   = -7,  /* device allocation failed              */
-    PGPU_ERR_BVH_INVALID     = -8,  /* node table is not a valid DFS tree    */
-    PGPU_ERR_DEVICE_STATUS   = -9   /* a kernel reported an internal error   */
+    PGPU_ERR_BVH_INVALID     = -8   /* node table is not a valid DFS tree    */
 };
 
 /* ---- scene description ------------------------------------------------- */
@@ -283,6 +283,16 @@ const char* pgpu_last_error(const pgpu_ctx* ctx);
 int32_t pgpu_set_stream(pgpu_ctx* ctx, void* cuda_stream);
 void*   pgpu_get_stream(pgpu_ctx* ctx);
 
+/* Wall-clock budget, in milliseconds, of the device work of one render,
+ * batch or adjoint call (0, the default: none). A call whose kernels have
+ * not finished within it returns PGPU_ERR_TIMEOUT before anything is copied
+ * to the caller's host buffers (device outputs are still written as the
+ * work completes); the context's next call first waits for that work. The
+ * kernels themselves always end: none waits on a flag or on another block.
+ * Counterpart of the reference's socket timeouts for workers that stop
+ * answering (src/distributed.hpp:527-545). */
+int32_t pgpu_set_timeout(pgpu_ctx* ctx, int32_t ms);
+
 /* Build the primitive's stored state from its constructor arguments, with
  * the same float arithmetic as the C++ constructors (plane normal and
  * cylinder/cone axis normalised; cylinder height halved).
@@ -341,6 +351,17 @@ int32_t pgpu_get_scene_info(pgpu_ctx* ctx, int32_t scene_id, pgpu_scene_info* ou
 int32_t pgpu_render(pgpu_ctx* ctx, int32_t scene_id,
                     const pgpu_render_params* params,
                     float* out_rgb, float* out_m2, pgpu_stats* stats);
+
+/* Render the window [x, x+w) x [y, y+h) of the image `params` describes:
+ * every pixel is seeded, jittered and traced as in pgpu_render of the whole
+ * image (the same values, bit for bit); out_rgb / out_m2 get w*h*3 floats,
+ * row-major. A frame split into windows over several GPUs (tiles, rows) is
+ * the fixed-frame counterpart of Pencil's tile farm, whose workers render
+ * 64x64 tiles of the frame (src/distributed.hpp:642-718, 380-434). */
+int32_t pgpu_render_window(pgpu_ctx* ctx, int32_t scene_id,
+                           const pgpu_render_params* params, int32_t x, int32_t y,
+                           int32_t w, int32_t h, float* out_rgb, float* out_m2,
+                           pgpu_stats* stats);
 
 /* Render several (scene, params) jobs of uneven size in one persistent
  * wavefront launch sequence. outs[i] receives job i's image. */

@@ -333,6 +333,17 @@ static int hit_prim(const pgpu_prim* pr, ray_t r, float tmin, float tmax, hitrec
     }
 }
 
+/* Bytes of a primitive's record as the GPU tables hold it (counters only). */
+static int prim_bytes(const pgpu_prim* pr) {
+    switch (pr->type) {
+        case PGPU_PRIM_SPHERE:   return 16;
+        case PGPU_PRIM_TRIANGLE: return 36;
+        case PGPU_PRIM_CUBE:     return 16;
+        case PGPU_PRIM_PLANE:    return 24;
+        default:                 return 32;
+    }
+}
+
 /* ---- BVH (src/bvh.hpp:31-48, AABB::hit src/primitives.hpp:38-49) -------- */
 static int box_hit(const pgpu_bvh_node* nd, ray_t r, float tmin, float tmax) {
     for (int a = 0; a < 3; ++a) {
@@ -357,7 +368,10 @@ static int node_hit(const trav_t* tv, int idx, ray_t r, float tmin, float tmax, 
     if (tv->cnt) tv->cnt[ORC_CNT_NODE_VISITS]++;
     if (!box_hit(nd, r, tmin, tmax)) return 0;
     if (nd->left < 0) {
-        if (tv->cnt) tv->cnt[ORC_CNT_PRIM_TESTS]++;
+        if (tv->cnt) {
+            tv->cnt[ORC_CNT_PRIM_TESTS]++;
+            tv->cnt[ORC_CNT_PRIM_BYTES] += (uint64_t)prim_bytes(&tv->s->prims[nd->right]);
+        }
         int ok = hit_prim(&tv->s->prims[nd->right], r, tmin, tmax, h);
         if (ok) h->prim = nd->right;
         return ok;
@@ -373,7 +387,10 @@ static int node_occ(const trav_t* tv, int idx, ray_t r, float tmin, float tmax) 
     if (!box_hit(nd, r, tmin, tmax)) return 0;
     if (nd->left < 0) {
         hitrec tmp;
-        if (tv->cnt) tv->cnt[ORC_CNT_PRIM_TESTS]++;
+        if (tv->cnt) {
+            tv->cnt[ORC_CNT_PRIM_TESTS]++;
+            tv->cnt[ORC_CNT_PRIM_BYTES] += (uint64_t)prim_bytes(&tv->s->prims[nd->right]);
+        }
         return hit_prim(&tv->s->prims[nd->right], r, tmin, tmax, &tmp);
     }
     if (node_occ(tv, nd->left, r, tmin, tmax)) return 1;
@@ -382,15 +399,32 @@ static int node_occ(const trav_t* tv, int idx, ray_t r, float tmin, float tmax) 
 }
 
 /* Scene::hit / Scene::occluded (src/scene.hpp:55-81), BVH branch. */
+/* The work of one walk, added to the counters of its kind. */
+static void split_counts(uint64_t* cnt, const uint64_t before[3], int nodes, int prims,
+                         int bytes) {
+    cnt[nodes] += cnt[ORC_CNT_NODE_VISITS] - before[0];
+    cnt[prims] += cnt[ORC_CNT_PRIM_TESTS] - before[1];
+    cnt[bytes] += cnt[ORC_CNT_PRIM_BYTES] - before[2];
+}
 static int scene_hit(const trav_t* tv, ray_t r, float tmin, float tmax, hitrec* h) {
     if (tv->cnt) tv->cnt[ORC_CNT_EXTENSION_RAYS]++;
     if (tv->s->n_nodes <= 0) return 0;
-    return node_hit(tv, 0, r, tmin, tmax, h);
+    if (!tv->cnt) return node_hit(tv, 0, r, tmin, tmax, h);
+    const uint64_t before[3] = {tv->cnt[ORC_CNT_NODE_VISITS], tv->cnt[ORC_CNT_PRIM_TESTS],
+                                tv->cnt[ORC_CNT_PRIM_BYTES]};
+    int ok = node_hit(tv, 0, r, tmin, tmax, h);
+    split_counts(tv->cnt, before, ORC_CNT_EXT_NODES, ORC_CNT_EXT_PRIMS, ORC_CNT_EXT_PRIM_BYTES);
+    return ok;
 }
 static int scene_occ(const trav_t* tv, ray_t r, float tmin, float tmax) {
     if (tv->cnt) tv->cnt[ORC_CNT_SHADOW_RAYS]++;
     if (tv->s->n_nodes <= 0) return 0;
-    return node_occ(tv, 0, r, tmin, tmax);
+    if (!tv->cnt) return node_occ(tv, 0, r, tmin, tmax);
+    const uint64_t before[3] = {tv->cnt[ORC_CNT_NODE_VISITS], tv->cnt[ORC_CNT_PRIM_TESTS],
+                                tv->cnt[ORC_CNT_PRIM_BYTES]};
+    int ok = node_occ(tv, 0, r, tmin, tmax);
+    split_counts(tv->cnt, before, ORC_CNT_SH_NODES, ORC_CNT_SH_PRIMS, ORC_CNT_SH_PRIM_BYTES);
+    return ok;
 }
 
 /* ---- camera (src/camera.hpp:67-86, src/camera.cpp:48-68) ---------------- */

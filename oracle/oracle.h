@@ -52,7 +52,18 @@ enum orc_counter {
     ORC_CNT_SHADOW_RAYS    = 2,   /* Scene::occluded calls                 */
     ORC_CNT_NODE_VISITS    = 3,   /* BVH nodes whose box was tested        */
     ORC_CNT_PRIM_TESTS     = 4,   /* primitive hit tests                   */
-    ORC_CNT_N              = 5
+    /* The same work split by kind of traversal, and the bytes of the
+     * primitive records tested (sphere 16 B = center + radius, triangle
+     * 36 B = three float3 vertices, cube 16 B, plane 24 B, cylinder and
+     * cone 32 B): the algorithmic traffic of a reference-order walk. */
+    ORC_CNT_EXT_NODES      = 5,   /* node visits by Scene::hit             */
+    ORC_CNT_EXT_PRIMS      = 6,   /* primitive tests by Scene::hit         */
+    ORC_CNT_EXT_PRIM_BYTES = 7,
+    ORC_CNT_SH_NODES       = 8,   /* node visits by Scene::occluded        */
+    ORC_CNT_SH_PRIMS       = 9,
+    ORC_CNT_SH_PRIM_BYTES  = 10,
+    ORC_CNT_PRIM_BYTES     = 11,  /* primitive bytes, both kinds           */
+    ORC_CNT_N              = 12
 };
 
 void orc_camera_basis(const pgpu_camera* cam, float out[21]);

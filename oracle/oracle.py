@@ -25,6 +25,9 @@ sys.path.insert(0, str(HERE.parent))
 from pencil_b200 import _abi as A  # noqa: E402
 
 CNT_REFERENCE_RAYS, CNT_EXTENSION_RAYS, CNT_SHADOW_RAYS, CNT_NODE_VISITS, CNT_PRIM_TESTS = range(5)
+(CNT_EXT_NODES, CNT_EXT_PRIMS, CNT_EXT_PRIM_BYTES, CNT_SH_NODES, CNT_SH_PRIMS,
+ CNT_SH_PRIM_BYTES, CNT_PRIM_BYTES) = range(5, 12)
+CNT_N = 12
 
 
 class OrcScene(C.Structure):
@@ -114,7 +117,7 @@ class Oracle:
         x, y, w, h = window if window is not None else (0, 0, settings.width, settings.height)
         out = np.zeros((h, w, 3), np.float32)
         m2 = np.zeros_like(out) if want_m2 else None
-        cnt = np.zeros(5, np.uint64)
+        cnt = np.zeros(CNT_N, np.uint64)
         win = np.asarray([x, y, w, h], np.int32)
         rc = fn(C.byref(self.s), C.byref(p), A.ptr(win), A.ptr(out), A.ptr(m2),
                 threads or os.cpu_count() or 1, A.ptr(cnt))
@@ -164,7 +167,7 @@ class Oracle:
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
         n = len(rays)
         prim, t = np.empty(n, np.int32), np.empty(n, np.float32)
-        cnt = np.zeros(5, np.uint64)
+        cnt = np.zeros(CNT_N, np.uint64)
         self.lib.orc_trace_rays(C.byref(self.s), A.ptr(rays), n, A.ptr(prim), A.ptr(t),
                                 A.ptr(cnt) if counters else None)
         return (prim, t, cnt) if counters else (prim, t)

@@ -24,7 +24,6 @@ ERR_TIMEOUT = -5
 ERR_NO_SCENE = -6
 ERR_OUT_OF_MEMORY = -7
 ERR_BVH_INVALID = -8
-ERR_DEVICE_STATUS = -9
 
 PRIM_SPHERE, PRIM_TRIANGLE, PRIM_CUBE, PRIM_PLANE, PRIM_CYLINDER, PRIM_CONE = range(6)
 MAT_DIFFUSE, MAT_METAL, MAT_DIELECTRIC = range(3)
@@ -114,6 +113,7 @@ EXPORTS = {
     "pgpu_last_error": (C.c_char_p, [C.c_void_p]),
     "pgpu_set_stream": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "pgpu_get_stream": (C.c_void_p, [C.c_void_p]),
+    "pgpu_set_timeout": (C.c_int32, [C.c_void_p, C.c_int32]),
     "pgpu_make_prim": (C.c_int32, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_float, C.c_float, C.c_void_p]),
     "pgpu_build_bvh": (C.c_int32, [C.POINTER(SceneDesc), C.c_void_p, C.POINTER(C.c_int32),
@@ -122,6 +122,9 @@ EXPORTS = {
     "pgpu_free_scene": (C.c_int32, [C.c_void_p, C.c_int32]),
     "pgpu_render": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(RenderParams), C.c_void_p,
                                 C.c_void_p, C.POINTER(Stats)]),
+    "pgpu_render_window": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(RenderParams),
+                                       C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                       C.c_void_p, C.POINTER(Stats)]),
     "pgpu_render_batch": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.POINTER(Stats)]),
     "pgpu_trace_rays": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,

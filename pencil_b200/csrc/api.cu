@@ -13,6 +13,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "host_internal.h"
@@ -20,8 +21,7 @@
 namespace pgpu {
 
 cudaError_t launch_megakernel(const SceneView& S, const RenderCfg& c, float* out, float* m2,
-                              unsigned long long* counters, cudaStream_t st,
-                              const int* tile = nullptr);
+                              unsigned long long* counters, cudaStream_t st);
 cudaError_t launch_query(const SceneView& S, bool camera, const float* in, int n, int* prim,
                          float* t, cudaStream_t st);
 
@@ -151,6 +151,10 @@ struct pgpu_ctx {
     std::vector<int2> ws_size_height;
     std::vector<char> ws_seen;
     WideScratch ws_collapse;
+    // wall-clock budget of a render's device work (pgpu_set_timeout; 0: none)
+    // and whether work of a call that ran out of it may still be running
+    int timeout_ms = 0;
+    bool in_flight = false;
 };
 
 namespace {
@@ -170,6 +174,45 @@ int fail(pgpu_ctx* c, int code, const char* fmt, ...) {
 int cuda_fail(pgpu_ctx* c, cudaError_t e, const char* what) {
     return fail(c, PGPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
+
+// Waits for the device work recorded by c->ev1 when the context has a time
+// budget: polls the event against the wall clock and, once the budget is
+// spent, returns PGPU_ERR_TIMEOUT without waiting further (nothing has been
+// copied to the caller's host buffers yet). The kernels themselves always
+// end -- no kernel waits on a flag -- and the context's next call waits for
+// them first (drain). Without a budget the caller's synchronize waits.
+int wait_render(pgpu_ctx* c) {
+    if (c->timeout_ms <= 0) return PGPU_OK;
+    const auto t0 = std::chrono::steady_clock::now();
+    while (true) {
+        const cudaError_t e = cudaEventQuery(c->ev1);
+        if (e == cudaSuccess) return PGPU_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(c, e, "waiting for the render");
+        const double ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                .count();
+        if (ms >= c->timeout_ms) {
+            c->in_flight = true;
+            return fail(c, PGPU_ERR_TIMEOUT,
+                        "device work did not finish within the %d ms budget (pgpu_set_timeout)",
+                        c->timeout_ms);
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+// The first thing a call that uses the context's stream does: wait for work
+// left running by a call that ran out of its time budget.
+int drain(pgpu_ctx* c) {
+    if (!c->in_flight) return PGPU_OK;
+    c->in_flight = false;
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? PGPU_OK : cuda_fail(c, e, "waiting for earlier device work");
+}
+#define PGPU_DRAIN(c)                          \
+    do {                                       \
+        if (int drc_ = drain(c)) return drc_;  \
+    } while (0)
 
 // f(begin, end) over [0, n) on the host worker threads (one when n is small).
 template <class F>
@@ -386,11 +429,19 @@ const char* pgpu_last_error(const pgpu_ctx* c) { return c ? c->err.c_str() : "nu
 
 int32_t pgpu_set_stream(pgpu_ctx* c, void* stream) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own;
     return PGPU_OK;
 }
 
 void* pgpu_get_stream(pgpu_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int32_t pgpu_set_timeout(pgpu_ctx* c, int32_t ms) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    if (ms < 0) return fail(c, PGPU_ERR_INVALID_ARG, "negative timeout %d ms", ms);
+    c->timeout_ms = ms;
+    return PGPU_OK;
+}
 
 int32_t pgpu_make_prim(int32_t type, int32_t material, const float* a, const float* b,
                        const float* cc, float s0, float s1, pgpu_prim* out) {
@@ -421,6 +472,7 @@ int32_t pgpu_build_bvh(const pgpu_scene* s, pgpu_bvh_node* out_nodes, int32_t* o
 int32_t pgpu_build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node* out_nodes,
                               int32_t* out_n_nodes, int32_t* out_depth) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     if (!s || !out_n_nodes || (s->n_prims > 0 && !s->prims) || s->n_prims < 0 ||
         s->n_mesh_triangles < 0 || s->n_mesh_vertices < 0 ||
         (s->n_mesh_triangles > 0 && (!s->mesh_indices || !s->mesh_vertices)))
@@ -458,6 +510,7 @@ int32_t pgpu_build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node* o
 
 int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     if (!s || !out_id) return fail(c, PGPU_ERR_INVALID_ARG, "null scene or id pointer");
     if (s->n_prims < 0 || s->n_mesh_triangles < 0 || s->n_materials < 0 || s->n_lights < 0 ||
         s->n_nodes < 0 || s->n_mesh_vertices < 0)
@@ -791,6 +844,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
 
 int32_t pgpu_free_scene(pgpu_ctx* c, int32_t id) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
     // work on the context stream that reads the scene finishes first; the
@@ -804,6 +858,7 @@ int32_t pgpu_free_scene(pgpu_ctx* c, int32_t id) {
 
 int32_t pgpu_get_scene_info(pgpu_ctx* c, int32_t id, pgpu_scene_info* out) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     if (!out) return fail(c, PGPU_ERR_INVALID_ARG, "null info pointer");
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
@@ -821,6 +876,7 @@ int32_t pgpu_get_scene_info(pgpu_ctx* c, int32_t id, pgpu_scene_info* out) {
 int32_t pgpu_tonemap(pgpu_ctx* c, const float* hdr, int32_t n_pixels, int32_t tonemap,
                      float exposure, int32_t flags, uint8_t* out_rgb8) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     if (!hdr || !out_rgb8 || n_pixels < 0)
         return fail(c, PGPU_ERR_INVALID_ARG, "null buffer or negative pixel count");
     if (tonemap < 0 || tonemap > 2)
@@ -857,6 +913,7 @@ int32_t pgpu_tonemap(pgpu_ctx* c, const float* hdr, int32_t n_pixels, int32_t to
 
 int32_t pgpu_update_materials(pgpu_ctx* c, int32_t id, const pgpu_material* m, int32_t n) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
     if (!m || n != ds->n_materials)
@@ -934,6 +991,8 @@ int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, Re
     if (p->block_size != 0 && p->block_size != 64 && p->block_size != 128 && p->block_size != 256)
         return fail(c, PGPU_ERR_INVALID_ARG, "block_size must be 0, 64, 128 or 256");
     cfg.block = p->block_size;
+    cfg.win[0] = cfg.win[1] = cfg.win[2] = cfg.win[3] = 0;
+    cfg.worker = false;
     (void)ds;
     return PGPU_OK;
 }
@@ -966,23 +1025,28 @@ int run_wavefront(pgpu_ctx* c, const std::vector<DeviceScene*>& scenes,
     return PGPU_OK;
 }
 
-}  // namespace pgpu
-
-extern "C" {
-
-int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float* out_rgb,
-                    float* out_m2, pgpu_stats* stats) {
+// pgpu_render and pgpu_render_window: the image, or the window `win` of it.
+static int32_t render_impl(pgpu_ctx* c, int32_t id, const pgpu_render_params* p,
+                           const int32_t* win, float* out_rgb, float* out_m2, pgpu_stats* stats) {
     auto t0 = std::chrono::steady_clock::now();
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
     if (!out_rgb) return fail(c, PGPU_ERR_INVALID_ARG, "null output");
     RenderCfg cfg;
     int rc = make_cfg(c, ds, p, cfg);
     if (rc) return rc;
+    if (win) {
+        if (win[2] <= 0 || win[3] <= 0 || win[0] < 0 || win[1] < 0 || win[0] + win[2] > cfg.W ||
+            win[1] + win[3] > cfg.H)
+            return fail(c, PGPU_ERR_INVALID_ARG, "window %d,%d %dx%d outside the %dx%d image",
+                        win[0], win[1], win[2], win[3], cfg.W, cfg.H);
+        for (int k = 0; k < 4; ++k) cfg.win[k] = win[k];
+    }
     PGPU_CUDA(c, cudaSetDevice(c->device));
     const bool dev_out = (p->flags & PGPU_FLAG_DEVICE_OUTPUT) != 0;
-    const size_t n3 = (size_t)cfg.W * cfg.H * 3;
+    const size_t n3 = (size_t)cfg.pixels() * 3;
     float* d_out = dev_out ? out_rgb : nullptr;
     float* d_m2 = dev_out ? out_m2 : nullptr;
     if (!dev_out) {
@@ -1009,6 +1073,7 @@ int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float*
         if (rc) return rc;
     }
     PGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    if ((rc = wait_render(c))) return rc;
     if (!dev_out) {
         PGPU_CUDA(c, cudaMemcpyAsync(out_rgb, d_out, n3 * 4, cudaMemcpyDeviceToHost, c->stream));
         if (out_m2)
@@ -1025,7 +1090,7 @@ int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float*
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         stats->device_ms = ms;
-        stats->paths = (uint64_t)cfg.W * cfg.H * cfg.spp;
+        stats->paths = (uint64_t)cfg.pixels() * cfg.spp;
         stats->extension_rays = cnt[CNT_EXT];
         stats->shadow_rays = cnt[CNT_SHADOW];
         stats->reference_rays = cnt[CNT_REF];
@@ -1044,9 +1109,26 @@ int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float*
     return PGPU_OK;
 }
 
+}  // namespace pgpu
+
+extern "C" {
+
+int32_t pgpu_render(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, float* out_rgb,
+                    float* out_m2, pgpu_stats* stats) {
+    return render_impl(c, id, p, nullptr, out_rgb, out_m2, stats);
+}
+
+int32_t pgpu_render_window(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, int32_t x,
+                           int32_t y, int32_t w, int32_t h, float* out_rgb, float* out_m2,
+                           pgpu_stats* stats) {
+    const int32_t win[4] = {x, y, w, h};
+    return render_impl(c, id, p, win, out_rgb, out_m2, stats);
+}
+
 int32_t pgpu_render_tile(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, int32_t tile_x,
                          int32_t tile_y, int32_t tile_w, int32_t tile_h, float* out_rgb) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
     if (!out_rgb) return fail(c, PGPU_ERR_INVALID_ARG, "null output");
@@ -1068,8 +1150,12 @@ int32_t pgpu_render_tile(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, i
         if ((rc = ensure(c, c->d_out, c->out_cap, n3 * 4))) return rc;
         d_out = c->d_out;
     }
-    const int tile[4] = {tile_x, tile_y, tile_w, tile_h};
-    cudaError_t e = launch_megakernel(ds->view, cfg, d_out, nullptr, c->d_cnt, c->stream, tile);
+    cfg.win[0] = tile_x;
+    cfg.win[1] = tile_y;
+    cfg.win[2] = tile_w;
+    cfg.win[3] = tile_h;
+    cfg.worker = true;
+    cudaError_t e = launch_megakernel(ds->view, cfg, d_out, nullptr, c->d_cnt, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "megakernel launch");
     if (!dev_out)
         PGPU_CUDA(c, cudaMemcpyAsync(out_rgb, d_out, n3 * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1081,6 +1167,7 @@ int32_t pgpu_render_batch(pgpu_ctx* c, int32_t n_jobs, const int32_t* ids,
                           const pgpu_render_params* params, float* const* outs, pgpu_stats* stats) {
     auto t0 = std::chrono::steady_clock::now();
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     if (n_jobs <= 0 || !ids || !params || !outs)
         return fail(c, PGPU_ERR_INVALID_ARG, "bad batch arguments");
     std::vector<DeviceScene*> scenes(n_jobs);
@@ -1123,6 +1210,7 @@ int32_t pgpu_render_batch(pgpu_ctx* c, int32_t n_jobs, const int32_t* ids,
                            &launches, prof ? kms : nullptr);
     if (rc) return rc;
     PGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    if ((rc = wait_render(c))) return rc;
     if (!dev_out)
         for (int k = 0; k < n_jobs; ++k)
             PGPU_CUDA(c, cudaMemcpyAsync(outs[k], d_outs[k], (size_t)cfgs[k].W * cfgs[k].H * 12,
@@ -1160,6 +1248,7 @@ int32_t pgpu_adjoint(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, const
                      pgpu_stats* stats) {
     auto t0 = std::chrono::steady_clock::now();
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
     if (!dl || !d_albedo || !d_emission || (!d_light && !ds->lights.empty()))
@@ -1193,6 +1282,7 @@ int32_t pgpu_adjoint(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, const
                                    out_rgb ? d_img : nullptr, c->d_cnt, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "adjoint launch");
     PGPU_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    if ((rc = wait_render(c))) return rc;
     PGPU_CUDA(c, cudaMemcpyAsync(d_albedo, d_g, nm * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     PGPU_CUDA(c, cudaMemcpyAsync(d_emission, d_g + 3 * nm, nm * 3 * sizeof(double),
                                  cudaMemcpyDeviceToHost, c->stream));
@@ -1224,6 +1314,7 @@ int32_t pgpu_adjoint(pgpu_ctx* c, int32_t id, const pgpu_render_params* p, const
 static int32_t run_query(pgpu_ctx* c, int32_t id, bool camera, const float* in, int32_t n,
                          int32_t* prim, float* t) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);
     if (n < 0 || (n > 0 && (!in || !prim || !t))) return fail(c, PGPU_ERR_INVALID_ARG, "bad query");
@@ -1266,6 +1357,7 @@ int32_t pgpu_primary_hits(pgpu_ctx* c, int32_t id, const float* uv, int32_t n, i
 extern "C" int32_t pgpu_render_noalloc(pgpu_ctx* c, int32_t id, const pgpu_render_params* p,
                                        float* out_rgb_device, float* out_m2_device) {
     if (!c) return PGPU_ERR_INVALID_ARG;
+    PGPU_DRAIN(c);
     if (c->err.capacity() < 512) c->err.reserve(512);
     DeviceScene* ds = find_scene(c, id);
     if (!ds) return fail(c, PGPU_ERR_NO_SCENE, "unknown scene id %d", id);

@@ -55,6 +55,9 @@ struct RenderCfg {
     bool mis;         // trace_path_mis's light weights
     bool binary_tree; // megakernel: Pencil's binary tree instead of the 4-wide tree
     int block;        // wavefront threads per block (0: the default)
+    int win[4];       // window x, y, w, h of the image (w = 0: the whole image)
+    bool worker;      // the distributed worker's jitter (render_tile)
+    long long pixels() const { return win[2] > 0 ? (long long)win[2] * win[3] : (long long)W * H; }
 };
 
 // Device counters written by the kernels (atomic adds).

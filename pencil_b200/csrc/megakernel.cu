@@ -47,7 +47,7 @@ mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __re
             for (int sy = 0; sy < P.n; ++sy) {
                 for (int sx = 0; sx < P.n; ++sx) {
                     float u, v;
-                    sample_uv(i, j, sx, sy, P.W, P.H, P.n, rng, u, v, tile);
+                    sample_uv(i, j, sx, sy, P.W, P.H, P.n, rng, u, v, P.worker != 0);
                     V3 c = tr.template sample<TREE>(camera_ray(S.cam, u, v), rng);
                     acc = acc + c;
                     acc2 = acc2 + c * c;
@@ -57,7 +57,7 @@ mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __re
             for (int s = lane_g; s < P.spp; s += G) {
                 Rng rng{path_seed(i, j, s + P.sample_offset, P.salt)};
                 float u, v;
-                sample_uv(i, j, s % P.n, s / P.n, P.W, P.H, P.n, rng, u, v, tile);
+                sample_uv(i, j, s % P.n, s / P.n, P.W, P.H, P.n, rng, u, v, P.worker != 0);
                 V3 c = tr.template sample<TREE>(camera_ray(S.cam, u, v), rng);
                 acc = acc + c;
                 acc2 = acc2 + c * c;
@@ -108,15 +108,10 @@ static cudaError_t launch_mk(const SceneView& S, const PathParams& P, int G, flo
 }
 
 cudaError_t launch_megakernel(const SceneView& S, const RenderCfg& c, float* out, float* m2,
-                              unsigned long long* counters, cudaStream_t st, const int* tile) {
+                              unsigned long long* counters, cudaStream_t st) {
     PathParams P{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias, c.salt,
-                 c.sample_offset, c.mis ? 1 : 0, 0, 0, 0, 0};
-    if (tile) {
-        P.tile_x = tile[0];
-        P.tile_y = tile[1];
-        P.tile_w = tile[2];
-        P.tile_h = tile[3];
-    }
+                 c.sample_offset, c.mis ? 1 : 0, c.win[0], c.win[1], c.win[2], c.win[3],
+                 c.worker ? 1 : 0};
     const bool seq = c.rng == PGPU_RNG_PIXEL_SEQUENTIAL;
     const bool tree = c.glass == PGPU_GLASS_BOTH_BRANCHES;
     int G = 1;

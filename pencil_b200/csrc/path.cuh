@@ -16,10 +16,13 @@ struct PathParams {
     uint32_t salt;
     int sample_offset;
     int mis;          // 1: trace_path_mis's light weights (src/renderer.hpp:1205-1346)
-    // A tile of the W x H image (tile_w > 0): the distributed worker's
-    // render_tile (src/distributed.hpp:380-434) -- pixels of the full image,
-    // jitter of half a pixel instead of half a sub-pixel.
+    // A window of the W x H image (tile_w > 0): pixels [tile_x, tile_x +
+    // tile_w) x [tile_y, tile_y + tile_h), each seeded and placed as in the
+    // full image; the output holds the window's pixels.
     int tile_x, tile_y, tile_w, tile_h;
+    // 1: the distributed worker's render_tile (src/distributed.hpp:380-434),
+    // whose jitter is half a pixel instead of half a sub-pixel
+    int worker;
 };
 
 enum { kModePT = 0, kModeWhitted = 1 };

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -252,7 +253,9 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
         long long local = path - J.path_off;
         int pix = (int)(local / P.spp);
         int s = (int)(local % P.spp);
-        int i = pix % P.W, j = pix / P.W;
+        // pixel of the image (of the job's window when it has one)
+        const int ww = P.tile_w > 0 ? P.tile_w : P.W;
+        int i = pix % ww + P.tile_x, j = pix / ww + P.tile_y;
         Rng rng{path_seed(i, j, s + P.sample_offset, P.salt)};
         float u, v;
         sample_uv(i, j, s % P.n, s / P.n, P.W, P.H, P.n, rng, u, v);
@@ -1071,7 +1074,8 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         long long slots = 0, pixels = 0;
         while (ji < n_jobs) {
             const WfJob& J = jobs[ji];
-            long long npix = (long long)J.P.W * J.P.H;
+            long long npix = J.P.tile_w > 0 ? (long long)J.P.tile_w * J.P.tile_h
+                                            : (long long)J.P.W * J.P.H;
             long long room = (Qeff - slots) / J.P.spp;
             long long take = std::min(room, npix - pix_in_job);
             if (take <= 0) break;
@@ -1182,15 +1186,16 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
         const RenderCfg& c = cfgs[k];
         WfJob& J = jobs[k];
         J.P = PathParams{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias,
-                         c.salt, c.sample_offset, c.mis ? 1 : 0};
+                         c.salt, c.sample_offset, c.mis ? 1 : 0, c.win[0], c.win[1], c.win[2],
+                         c.win[3], 0};
         J.view = job_view[k];
         J.path_off = path_off;
         J.pix_off = pix_off;
         J.G = lanes_for(c.spp);
         J.out = outs[k];
         J.m2 = m2s[k];
-        path_off += (long long)c.W * c.H * c.spp;
-        pix_off += (long long)c.W * c.H;
+        path_off += c.pixels() * c.spp;
+        pix_off += c.pixels();
         iters = std::max(iters, c.depth);
         max_spp = std::max(max_spp, c.spp);
         maxS = std::max(maxS, max_shadow_records(views[J.view], lights[J.view], c.soft));
@@ -1202,6 +1207,14 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
         packets = packets && c.packets;
     }
     total_paths = path_off;
+    // Fault injection, host side: PGPU_INJECT_SHADOW_RECORDS=k gives every
+    // path vertex room for only k shadow records, so that a scene needing
+    // more makes shade report the overflow (it stores no record beyond the
+    // room it has) and the call returns PGPU_ERR_QUEUE_OVERFLOW.
+    if (const char* inj = std::getenv("PGPU_INJECT_SHADOW_RECORDS")) {
+        const int k = std::atoi(inj);
+        if (k >= 1 && k < maxS) maxS = k;
+    }
     long long Q = qcap > 0 ? qcap : (1LL << 22);
     Q = std::max<long long>(Q, max_spp);
     Q = std::min<long long>(Q, total_paths);
@@ -1247,6 +1260,7 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     for (const auto& J : jobs) {
         mix((unsigned long long)J.P.W); mix((unsigned long long)J.P.H);
         mix((unsigned long long)J.P.spp); mix((unsigned long long)J.P.depth);
+        mix((unsigned long long)J.P.tile_w); mix((unsigned long long)J.P.tile_h);
     }
     mix((unsigned long long)iters);
     mix((unsigned long long)one);
@@ -1476,7 +1490,7 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
     A.refill_below = kDefaultRefill;
     WfJob J{};
     J.P = PathParams{c.W, c.H, c.n, c.spp, c.depth, c.mode, c.rng, c.glass, c.soft, c.bias,
-                     c.salt, c.sample_offset, c.mis ? 1 : 0};
+                     c.salt, c.sample_offset, c.mis ? 1 : 0, 0, 0, 0, 0, 0};
     J.view = 0;
     J.path_off = 0;
     J.pix_off = 0;

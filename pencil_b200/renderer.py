@@ -137,6 +137,10 @@ class GpuContext:
     def set_stream(self, stream: int | None) -> None:
         self.check(self.lib.pgpu_set_stream(self.h, stream), "pgpu_set_stream")
 
+    def set_timeout(self, ms: int) -> None:
+        """Wall-clock budget of a render's device work (0: none)."""
+        self.check(self.lib.pgpu_set_timeout(self.h, int(ms)), "pgpu_set_timeout")
+
     def upload(self, scene: Scene, nodes: np.ndarray | None = None,
                camera: CameraArgs | None = None) -> int:
         d, keep = scene.desc(nodes, camera)
@@ -205,6 +209,24 @@ class GpuContext:
         st = A.Stats()
         self.check(self.lib.pgpu_render(self.h, sid, C.byref(p), A.ptr(out), A.ptr(m2),
                                         C.byref(st)), "pgpu_render")
+        if stats is not None:
+            stats.fill(st)
+        return out
+
+    def render_window(self, sid: int, settings: RenderSettings,
+                      window: tuple[int, int, int, int], out: np.ndarray | None = None,
+                      m2: np.ndarray | None = None,
+                      stats: RenderStats | None = None) -> np.ndarray:
+        """The window (x, y, w, h) of the image `settings` describe: each
+        pixel as in the whole image's render."""
+        x, y, w, h = (int(v) for v in window)
+        p = settings.params()
+        if out is None:
+            out = np.empty((h, w, 3), np.float32)
+        assert out.dtype == np.float32 and out.size == w * h * 3
+        st = A.Stats()
+        self.check(self.lib.pgpu_render_window(self.h, sid, C.byref(p), x, y, w, h, A.ptr(out),
+                                               A.ptr(m2), C.byref(st)), "pgpu_render_window")
         if stats is not None:
             stats.fill(st)
         return out

@@ -49,8 +49,12 @@ def test_adjoint_matches_fp64_cpu_adjoint(gpu, case):
     gpu.free(sid)
 
 
-def test_adjoint_matches_central_differences(gpu):
-    w, target, first = W.adjoint_box(1000, 128, 128, 4, 6, seed=5)
+@pytest.mark.parametrize("res", [128, 512])
+def test_adjoint_matches_central_differences(gpu, res):
+    """Central differences with common random numbers (h = 1e-3, the same
+    seeds on both sides) on the box with 1,000 spheres, 16 spp, depth 6; at
+    512x512 this is the adjoint configuration itself."""
+    w, target, first = W.adjoint_box(1000, res, res, 4, 6, seed=5)
     scene, st = w.scene, w.settings
     sid = gpu.upload(scene)
     fwd = gpu.render(sid, st)

@@ -503,3 +503,28 @@ def test_full_size_mesh_primary_hits(gpu):
     assert np.array_equal(p, op) and np.array_equal(t.view(np.uint32), ot.view(np.uint32))
     assert (p >= w.scene.n_prims).mean() > 0.2       # rays that hit the mesh
     gpu.free(sid)
+
+
+@pytest.mark.parametrize("engine", [A.ENGINE_WAVEFRONT, A.ENGINE_MEGAKERNEL])
+def test_window_render_equals_the_crop_of_the_frame(gpu, scenes, engine):
+    """pgpu_render_window: every pixel of a window equals the same pixel of
+    the whole image's render, bit for bit (and its second moment), for
+    windows at the corners, inside and across the whole image; bands of rows
+    reassemble the frame (the fixed-frame multi-GPU split)."""
+    scene, fx, sid = scenes["prims_mix"]
+    st = settings_of(fx, True, engine=engine)
+    st.width, st.height = 70, 45
+    m2 = np.zeros((st.height, st.width, 3), np.float32)
+    full = gpu.render(sid, st, m2=m2)
+    for x, y, w, h in ((0, 0, 16, 9), (54, 36, 16, 9), (20, 11, 33, 17), (0, 0, 70, 45)):
+        wm2 = np.zeros((h, w, 3), np.float32)
+        win = gpu.render_window(sid, st, (x, y, w, h), m2=wm2)
+        assert np.array_equal(win.view(np.uint32), full[y:y + h, x:x + w].view(np.uint32))
+        assert np.array_equal(wm2.view(np.uint32), m2[y:y + h, x:x + w].view(np.uint32))
+    from pencil_b200.distributed import row_band
+    bands = [gpu.render_window(sid, st, (0, y0, st.width, y1 - y0))
+             for y0, y1 in (row_band(st.height, r, 3) for r in range(3))]
+    assert np.array_equal(np.concatenate(bands).view(np.uint32), full.view(np.uint32))
+    with pytest.raises(A.GpuError) as e:
+        gpu.render_window(sid, st, (60, 0, 16, 9))
+    assert e.value.code == A.ERR_INVALID_ARG
