@@ -325,6 +325,18 @@ int32_t pgpu_build_bvh_device(pgpu_ctx* ctx, const pgpu_scene* scene,
                               pgpu_bvh_node* out_nodes, int32_t* out_n_nodes,
                               int32_t* out_depth);
 
+/* Pencil's own SAH tree (BVH::build, src/bvh.hpp:74-192: 12 buckets along
+ * the longest axis, cost 1 + (nL SA_L + nR SA_R) / SA_P, median split for
+ * <= 4 primitives and when no bucket boundary separates) built on the GPU,
+ * one tree level at a time, in the same table format. Splits are those of
+ * the host build; the sides of a split keep their primitives in a stable
+ * order where Pencil's std::partition does not, so trees agree node for node
+ * unless two primitives tie in a median split's centroid key. out_nodes
+ * NULL: *out_n_nodes gets the table size only. */
+int32_t pgpu_build_bvh_device_sah(pgpu_ctx* ctx, const pgpu_scene* scene,
+                                  pgpu_bvh_node* out_nodes, int32_t* out_n_nodes,
+                                  int32_t* out_depth);
+
 /* Upload a scene; returns a scene id valid until pgpu_free_scene. */
 int32_t pgpu_upload_scene(pgpu_ctx* ctx, const pgpu_scene* scene,
                           int32_t* out_scene_id);

@@ -142,6 +142,8 @@ EXPORTS = {
                                      C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     "pgpu_build_bvh_device": (C.c_int32, [C.c_void_p, C.POINTER(SceneDesc), C.c_void_p,
                                           C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "pgpu_build_bvh_device_sah": (C.c_int32, [C.c_void_p, C.POINTER(SceneDesc), C.c_void_p,
+                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "pgpu_render_noalloc": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(RenderParams),
                                         C.c_void_p, C.c_void_p]),
 }

@@ -48,6 +48,8 @@ int adjoint_max_lights();
 cudaError_t launch_tonemap(const float* d_hdr, long long n_pixels, int mode, float exposure,
                            uint8_t* d_out, const float* d_thr, cudaStream_t st);
 const float* gamma_thresholds_host();
+cudaError_t device_sah(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_node>& out,
+                       int& depth, cudaStream_t st);
 cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_node>& out,
                         int& depth, cudaStream_t st);
 
@@ -469,8 +471,11 @@ int32_t pgpu_build_bvh(const pgpu_scene* s, pgpu_bvh_node* out_nodes, int32_t* o
     return PGPU_OK;
 }
 
-int32_t pgpu_build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node* out_nodes,
-                              int32_t* out_n_nodes, int32_t* out_depth) {
+}  // extern "C"
+
+// pgpu_build_bvh_device / _sah: `sah` selects Pencil's binned SAH, else the LBVH.
+static int32_t build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node* out_nodes,
+                                int32_t* out_n_nodes, int32_t* out_depth, bool sah) {
     if (!c) return PGPU_ERR_INVALID_ARG;
     PGPU_DRAIN(c);
     if (!s || !out_n_nodes || (s->n_prims > 0 && !s->prims) || s->n_prims < 0 ||
@@ -501,11 +506,24 @@ int32_t pgpu_build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node* o
     PGPU_CUDA(c, cudaSetDevice(c->device));
     std::vector<pgpu_bvh_node> nodes;
     int depth = 0;
-    cudaError_t e = device_lbvh(*s, n, nodes, depth, c->stream);
+    cudaError_t e = sah ? device_sah(*s, n, nodes, depth, c->stream)
+                        : device_lbvh(*s, n, nodes, depth, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "device BVH build");
     std::memcpy(out_nodes, nodes.data(), nodes.size() * sizeof(pgpu_bvh_node));
     if (out_depth) *out_depth = depth;
     return PGPU_OK;
+}
+
+extern "C" {
+
+int32_t pgpu_build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node* out_nodes,
+                              int32_t* out_n_nodes, int32_t* out_depth) {
+    return build_bvh_device(c, s, out_nodes, out_n_nodes, out_depth, false);
+}
+
+int32_t pgpu_build_bvh_device_sah(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node* out_nodes,
+                                  int32_t* out_n_nodes, int32_t* out_depth) {
+    return build_bvh_device(c, s, out_nodes, out_n_nodes, out_depth, true);
 }
 
 int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {

@@ -153,16 +153,17 @@ class GpuContext:
     def free(self, sid: int) -> None:
         self.check(self.lib.pgpu_free_scene(self.h, sid), "pgpu_free_scene")
 
-    def build_bvh_device(self, scene: Scene) -> tuple[np.ndarray, int]:
-        """A linear BVH built on the GPU, in the node-table format of
-        Scene.build_bvh (DFS pre-order); returns (nodes, depth)."""
+    def build_bvh_device(self, scene: Scene, method: str = "lbvh") -> tuple[np.ndarray, int]:
+        """A BVH built on the GPU, in the node-table format of
+        Scene.build_bvh (DFS pre-order): method "lbvh" a linear BVH, "sah"
+        Pencil's binned SAH tree. Returns (nodes, depth)."""
+        fn = {"lbvh": "pgpu_build_bvh_device", "sah": "pgpu_build_bvh_device_sah"}[method]
         d, keep = scene.desc()
         n = scene.n_unified
         nodes = np.zeros(max(2 * n - 1, 1), A.NODE_DTYPE)
         cnt, depth = C.c_int32(0), C.c_int32(0)
-        self.check(self.lib.pgpu_build_bvh_device(self.h, C.byref(d), A.ptr(nodes),
-                                                  C.byref(cnt), C.byref(depth)),
-                   "pgpu_build_bvh_device")
+        self.check(getattr(self.lib, fn)(self.h, C.byref(d), A.ptr(nodes), C.byref(cnt),
+                                         C.byref(depth)), fn)
         del keep
         return nodes[: cnt.value].copy(), depth.value
 
