@@ -416,7 +416,7 @@ int32_t pgpu_adjoint(pgpu_ctx* ctx, int32_t scene_id,
  * that must not stall on an allocation, or code that runs between
  * allocation-free phases of a larger pipeline. This entry point renders with
  * the wavefront engine over one file-scope device array of fixed size
- * (21.5 MiB: 65,536 paths in flight, processed chunk after chunk; every GPU
+ * (24.5 MiB: 65,536 paths in flight, processed chunk after chunk; every GPU
  * that loads the library holds it until exit). It calls no cudaMalloc,
  * cudaFree or other allocating routine; the scene must already be uploaded
  * and the outputs are caller-owned DEVICE buffers (out_rgb_device:

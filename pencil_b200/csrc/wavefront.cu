@@ -80,11 +80,14 @@ struct WfArgs {
     uint4* st;                // rng, depth, flags, job
     float4* hit;              // t, best ref, leaf slot, found
     float4* pb;               // Whitted vertex: pending base.xyz, scale s
-    float4* pt;               // pending tail.xyz, kind | shadow records << 2
     float4* pw;               // Whitted vertex: pending weight.xyz
-    float4* sh_o;             // [k * Q + slot] origin.xyz, tmin
-    float4* sh_d;             // direction.xyz, tmax
-    float4* sh_c;             // contribution.xyz, test | group_end << 1
+    // Shadow record k of a slot: one 64-byte block, [(k * Q + slot) * 4 + f],
+    //   f = 0 origin.xyz, tmin; 1 direction.xyz, tmax;
+    //       2 contribution.xyz, test | group_end << 1;
+    //       3 (block k = 0 only) the vertex's pending tail.xyz, kind | records << 2.
+    // The shadow kernel visits slots in sorted, not slot, order: a record it
+    // reads is two whole sectors, the pending word sharing the second.
+    float4* rec;
     int* q[2];                // queues: kOctants bins of Q entries each
     int* counts;              // [iteration * kOctants + bin]
     unsigned int* work;       // [iteration * 3 + kernel] fetch cursors
@@ -264,7 +267,7 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
         A.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
         A.T[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
         A.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        A.pt[slot] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));   // nothing pending
+        A.rec[(size_t)slot * 4 + 3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));  // nothing pending
         uint32_t flags = P.mode == kModeWhitted ? kFlagWhitted : 0u;
         A.st[slot] = make_uint4(rng.s, (unsigned)P.depth, flags, (unsigned)jb);
         if (COUNT) rc.ref++;
@@ -491,18 +494,19 @@ struct StoreNee {
             atomicOr(A.status, 1);
             return;
         }
-        size_t k = (size_t)n * A.Q + slot;
+        float4* b = A.rec + ((size_t)n * A.Q + slot) * 4;
         if (n == 0) { o0 = r.o; d0 = r.d; }
-        A.sh_o[k] = make_float4(r.o.x, r.o.y, r.o.z, tmin);
-        A.sh_d[k] = make_float4(r.d.x, r.d.y, r.d.z, tmax);
-        A.sh_c[k] = make_float4(c.x, c.y, c.z, __int_as_float((test ? 1 : 0) | (group_end << 1)));
+        b[0] = make_float4(r.o.x, r.o.y, r.o.z, tmin);
+        b[1] = make_float4(r.d.x, r.d.y, r.d.z, tmax);
+        b[2] = make_float4(c.x, c.y, c.z, __int_as_float((test ? 1 : 0) | (group_end << 1)));
         ++n;
     }
     __device__ __forceinline__ void pending(V3 tl, V3 ww, float ss) { tail = tl; w = ww; s = ss; }
     __device__ __forceinline__ void store() {
         // pt: tail and kind | records << 2; a Whitted vertex also needs its
         // base and scale (pb) and weight (pw)
-        A.pt[slot] = make_float4(tail.x, tail.y, tail.z, __int_as_float(kind | (n << 2)));
+        A.rec[(size_t)slot * 4 + 3] =
+            make_float4(tail.x, tail.y, tail.z, __int_as_float(kind | (n << 2)));
         if (kind == 2) {
             A.pb[slot] = make_float4(base.x, base.y, base.z, s);
             A.pw[slot] = make_float4(w.x, w.y, w.z, 0.0f);
@@ -728,13 +732,13 @@ wf_shadow(WfArgs A, int it) {
     // traversal (returns true) or all are done (pending terms applied).
     auto advance = [&]() -> bool {
         while (k < n) {
-            const size_t idx = (size_t)k * A.Q + slot;
-            const float4 sc = A.sh_c[idx];
+            const float4* b = A.rec + ((size_t)k * A.Q + slot) * 4;
+            const float4 sc = b[2];
             const int bits = __float_as_int(sc.w);
             c = v3(sc.x, sc.y, sc.z);
             group_end = bits >> 1;
             if (bits & 1) {
-                const float4 so = A.sh_o[idx], sd = A.sh_d[idx];
+                const float4 so = b[0], sd = b[1];
                 if (COUNT) rc.shadow++;
                 if (!tr.init(scene(), Ray{v3(so.x, so.y, so.z), v3(sd.x, sd.y, sd.z)}, so.w, sd.w,
                              &rc.tc))
@@ -745,7 +749,7 @@ wf_shadow(WfArgs A, int it) {
             }
             ++k;
         }
-        const float4 pt = A.pt[slot];
+        const float4 pt = A.rec[(size_t)slot * 4 + 3];
         V3 w = v3(0.0f, 0.0f, 0.0f);
         float sc = 0.0f;
         if (acc.kind == 2) {
@@ -770,7 +774,7 @@ wf_shadow(WfArgs A, int it) {
                 const int e = base + __popc(idle & below);
                 if (e < total) {
                     slot = sorted ? A.qs[e] : qv.slot(e);
-                    const int info = __float_as_int(A.pt[slot].w);
+                    const int info = __float_as_int(A.rec[(size_t)slot * 4 + 3].w);
                     const int kind = info & 3;
                     if (kind != 0) {
                         if constexpr (!ONE) S = &A.views[A.jobs[A.st[slot].w].view];
@@ -922,8 +926,8 @@ static cudaError_t ensure_scratch(WfScratch& W, int Q, int maxS, int iters, int 
     n_views = std::max(n_views, W.views_cap);
     size_t per = al((size_t)Q * 16);
     size_t sz = 0;
-    sz += 9 * per;                                   // ray_o ray_d T L st hit pb pt pw
-    sz += 3 * (size_t)maxS * per;                    // shadow records
+    sz += 8 * per;                                   // ray_o ray_d T L st hit pb pw
+    sz += 4 * (size_t)maxS * per;                    // shadow records (64 B each)
     sz += 2 * al((size_t)kOctants * Q * 4);          // queues
     sz += al((size_t)(iters + 2) * kOctants * 4);    // counts
     sz += al((size_t)(iters + 2) * 3 * 4);           // work cursors
@@ -954,11 +958,8 @@ static cudaError_t ensure_scratch(WfScratch& W, int Q, int maxS, int iters, int 
     A.st = reinterpret_cast<uint4*>(take((size_t)Q * 16));
     A.hit = reinterpret_cast<float4*>(take((size_t)Q * 16));
     A.pb = reinterpret_cast<float4*>(take((size_t)Q * 16));
-    A.pt = reinterpret_cast<float4*>(take((size_t)Q * 16));
     A.pw = reinterpret_cast<float4*>(take((size_t)Q * 16));
-    A.sh_o = reinterpret_cast<float4*>(take((size_t)maxS * Q * 16));
-    A.sh_d = reinterpret_cast<float4*>(take((size_t)maxS * Q * 16));
-    A.sh_c = reinterpret_cast<float4*>(take((size_t)maxS * Q * 16));
+    A.rec = reinterpret_cast<float4*>(take((size_t)maxS * Q * 64));
     A.q[0] = reinterpret_cast<int*>(take((size_t)kOctants * Q * 4));
     A.q[1] = reinterpret_cast<int*>(take((size_t)kOctants * Q * 4));
     A.counts = reinterpret_cast<int*>(take((size_t)(iters + 2) * kOctants * 4));
@@ -1386,8 +1387,8 @@ constexpr int kStaticMaxDepth = 64;       // bounces (iterations per chunk)
 constexpr size_t static_al(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kStaticArray = static_al((size_t)kStaticSlots * 16);
 constexpr size_t kStaticBytes =
-    9 * kStaticArray +                                           // path state
-    3 * (size_t)kStaticShadow * kStaticArray +                   // shadow records
+    8 * kStaticArray +                                           // path state
+    4 * (size_t)kStaticShadow * kStaticArray +                   // shadow records (64 B)
     2 * static_al((size_t)kStaticSlots * 4) +                    // queues (one bin each)
     static_al((size_t)(kStaticMaxDepth + 2) * kOctants * 4) +    // queue counts
     static_al((size_t)(kStaticMaxDepth + 2) * 3 * 4) +           // fetch cursors
@@ -1471,11 +1472,8 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
     A.st = reinterpret_cast<uint4*>(take((size_t)Q * 16));
     A.hit = reinterpret_cast<float4*>(take((size_t)Q * 16));
     A.pb = reinterpret_cast<float4*>(take((size_t)Q * 16));
-    A.pt = reinterpret_cast<float4*>(take((size_t)Q * 16));
     A.pw = reinterpret_cast<float4*>(take((size_t)Q * 16));
-    A.sh_o = reinterpret_cast<float4*>(take((size_t)kStaticShadow * Q * 16));
-    A.sh_d = reinterpret_cast<float4*>(take((size_t)kStaticShadow * Q * 16));
-    A.sh_c = reinterpret_cast<float4*>(take((size_t)kStaticShadow * Q * 16));
+    A.rec = reinterpret_cast<float4*>(take((size_t)kStaticShadow * Q * 64));
     A.q[0] = reinterpret_cast<int*>(take((size_t)Q * 4));
     A.q[1] = reinterpret_cast<int*>(take((size_t)Q * 4));
     A.counts = reinterpret_cast<int*>(take((size_t)(kStaticMaxDepth + 2) * kOctants * 4));
