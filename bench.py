@@ -565,51 +565,60 @@ def measure_extras(ctx, sid, st, img, stream) -> dict:
     return out
 
 
-def _once_ms(stream, fn) -> float:
-    """Device ms of one call of a long render (CUDA events around it)."""
-    import torch
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    fn()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1)
+def _reference_image(ctx, sid, st, window, frames: int = 64):
+    """Mean of `frames` renders of n=8 (64 spp) with distinct sample offsets,
+    and the relative RMSE of that mean's own noise (from its two halves)."""
+    from pencil_b200.renderer import RenderStats
+    halves = [np.zeros((window[3], window[2], 3)), np.zeros((window[3], window[2], 3))]
+    q = dataclasses.replace(st, samples=8)
+    ms = 0.0
+    for k in range(frames):
+        q.sample_offset = (k + 1000) * 64
+        s_ = RenderStats()
+        halves[k * 2 // frames] += ctx.render_window(sid, q, window, stats=s_)
+        ms += s_.device_ms
+    a, b = halves[0] / (frames // 2), halves[1] / (frames // 2)
+    ref = 0.5 * (a + b)
+    noise = float(np.sqrt(((a - b) ** 2).mean()) / 2 / ref.mean())
+    return ref, noise, ms
 
 
-def _rel_rmse(img, ref) -> float:
-    import torch
-    return float(torch.sqrt(((img - ref) ** 2).mean()) / ref.mean())
-
-
-def _equal_rmse_point(ctx, sid, st, ref, stream, target=0.01) -> dict:
+def _equal_rmse_point(ctx, sid, st, window, ref, noise, target=0.01) -> dict:
     """The samples per pixel at which the production estimator's image is
-    within `target` relative RMSE of `ref`, and the time of both engines to
-    render the frame at that point. The RMSE model e^2 = a/spp + b (b: the
-    reference's own noise) is fitted from renders at n=4 and n=16."""
-    import torch
+    within `target` relative RMSE of `ref`, and the device time of both
+    engines to render the window at that point. Model: e^2 = a / spp +
+    noise^2 (noise: the reference's own), a from a 16-spp render; the point
+    is raised until the measured e meets the target (n <= 64)."""
     from pencil_b200 import _abi as A
-    img = torch.empty_like(ref)
-    q = dataclasses.replace(st, engine=A.ENGINE_WAVEFRONT)
-    e = {}
-    for n in (4, 16):
-        q.samples = n
-        ctx.render_device(sid, q, img.data_ptr())
-        e[n] = _rel_rmse(img, ref)
-    a = (e[4] ** 2 - e[16] ** 2) / (1 / 16 - 1 / 256)
-    b = max(e[4] ** 2 - a / 16, 0.0)
-    out = {"rel_rmse_16spp": e[4], "rel_rmse_256spp": e[16], "reference_noise_rel_rmse": b ** 0.5}
-    if b >= target ** 2 or a <= 0:
+    from pencil_b200.renderer import RenderStats
+
+    def rmse(img):
+        return float(np.sqrt(((img - ref) ** 2).mean()) / ref.mean())
+
+    q = dataclasses.replace(st, engine=A.ENGINE_WAVEFRONT, samples=4)
+    e16 = rmse(ctx.render_window(sid, q, window))
+    a = 16.0 * max(e16 ** 2 - noise ** 2, 0.0)
+    out = {"rel_rmse_16spp": e16, "reference_noise_rel_rmse": noise}
+    if noise >= target or a <= 0.0:
         out["reachable"] = False
+        out["why"] = "the 4096-spp reference's own noise is above the target"
         return out
-    n = min(64, int(np.ceil(np.sqrt(a / (target ** 2 - b)))))
+    n = min(64, int(np.ceil(np.sqrt(a / (target ** 2 - noise ** 2)))))
     res = {}
-    for name, eng in (("wavefront", A.ENGINE_WAVEFRONT), ("megakernel", A.ENGINE_MEGAKERNEL)):
-        q = dataclasses.replace(st, engine=eng, samples=n)
-        ms = _once_ms(stream, lambda: ctx.render_device(sid, q, img.data_ptr()))
-        paths = q.width * q.height * n * n
-        res[name] = {"ms": ms, "mpaths_s": paths / ms / 1e3, "rel_rmse": _rel_rmse(img, ref)}
-    out.update({"reachable": True, "spp": n * n, "n": n, **res,
+    for _ in range(6):
+        res = {}
+        for name, eng in (("wavefront", A.ENGINE_WAVEFRONT), ("megakernel", A.ENGINE_MEGAKERNEL)):
+            q = dataclasses.replace(st, engine=eng, samples=n)
+            s_ = RenderStats()
+            img = ctx.render_window(sid, q, window, stats=s_)
+            paths = window[2] * window[3] * n * n
+            res[name] = {"ms": s_.device_ms, "mpaths_s": paths / s_.device_ms / 1e3,
+                         "rel_rmse": rmse(img)}
+        if res["wavefront"]["rel_rmse"] <= target or n >= 64:
+            break
+        n = min(64, n + 2)
+    out.update({"reachable": res["wavefront"]["rel_rmse"] <= target, "spp": n * n, "n": n,
+                **res,
                 "wavefront_over_megakernel": res["megakernel"]["ms"] / res["wavefront"]["ms"]})
     return out
 
@@ -618,60 +627,43 @@ def measure_quality(ctx, sid, st, stream) -> dict:
     """Image quality at the north star's operating point (relative RMSE <=
     1% against a 4096-spp reference).
 
-    Sphere cloud, the full frame: the reference image is the reference's
-    own estimator -- trace_path with both dielectric branches (the
-    megakernel's exact glass mode) -- at 4096 spp, rendered as 64 frames of
-    64 spp with distinct sample offsets. Mesh box (the displaced icosphere,
-    quad light): the frame at 256x256, reference 4096 spp of the production
-    estimator; the reference's own estimator (BSDF sampling only: the small
-    emitter is found by chance) is measured against it too."""
-    import torch
+    Sphere cloud, the 640x360 middle of the full 1280x720 frame (the dense
+    part of the cloud), rendered as windows of the frame: the reference
+    image is the reference's own estimator -- trace_path with both
+    dielectric branches (the megakernel's exact glass mode) -- at 4096 spp,
+    as 64 renders of 64 spp with distinct sample offsets. Mesh box (the
+    displaced icosphere, quad light) at 256x256: reference 4096 spp of the
+    production estimator; the reference's own estimator (BSDF sampling only:
+    the small emitter is found by chance) is measured against it too."""
     from pencil_b200 import _abi as A
     from pencil_b200 import workloads as W
     out = {}
-    ref = torch.zeros((st.height, st.width, 3), dtype=torch.float32, device="cuda")
-    img = torch.empty_like(ref)
-    q = dataclasses.replace(st, engine=A.ENGINE_MEGAKERNEL, glass=A.GLASS_BOTH_BRANCHES,
-                            samples=8)
-    frames = 64
+    window = (320, 180, 640, 360)
     t0 = time.perf_counter()
-    for k in range(frames):
-        q.sample_offset = (k + 1000) * 64
-        ctx.render_device(sid, q, img.data_ptr())
-        ref += img
-    ref /= frames
-    torch.cuda.synchronize()
-    out["sphere_cloud"] = {"reference": "trace_path with both glass branches, 4096 spp",
+    qref = dataclasses.replace(st, engine=A.ENGINE_MEGAKERNEL, glass=A.GLASS_BOTH_BRANCHES)
+    ref, noise, ref_ms = _reference_image(ctx, sid, qref, window)
+    out["sphere_cloud"] = {"window": list(window),
+                           "reference": "trace_path with both glass branches, 4096 spp",
                            "reference_seconds": time.perf_counter() - t0,
-                           **_equal_rmse_point(ctx, sid, st, ref, stream)}
+                           **_equal_rmse_point(ctx, sid, st, window, ref, noise)}
     # mesh box at 256x256
     wm = W.mesh_box(width=256, height=256)
     nodes, _ = wm.scene.build_bvh()
     sm = ctx.upload(wm.scene, nodes)
-    sm_st = wm.settings
-    mref = torch.zeros((256, 256, 3), dtype=torch.float32, device="cuda")
-    mimg = torch.empty_like(mref)
-    q = dataclasses.replace(sm_st, engine=A.ENGINE_WAVEFRONT, samples=8)
-    for k in range(frames):
-        q.sample_offset = (k + 1000) * 64
-        ctx.render_device(sm, q, mimg.data_ptr())
-        mref += mimg
-    mref /= frames
+    sm_st = dataclasses.replace(wm.settings, engine=A.ENGINE_WAVEFRONT)
+    mwin = (0, 0, 256, 256)
+    mref, mnoise, _ = _reference_image(ctx, sm, sm_st, mwin)
     rec = {"workload": "mesh_box at 256x256, depth 12",
            "reference": "production estimator (quad-light NEE), 4096 spp",
-           **_equal_rmse_point(ctx, sm, sm_st, mref, stream)}
+           **_equal_rmse_point(ctx, sm, sm_st, mwin, mref, mnoise)}
     # the reference's own estimator (no quad light: BSDF sampling only) at
     # 4096 spp against that image
     bs = wm.scene
     bs.lights = [l for l in bs.lights if l.kind != A.LIGHT_QUAD]
     sb = ctx.upload(bs, nodes)
-    acc = torch.zeros_like(mref)
-    for k in range(frames):
-        q.sample_offset = (k + 1000) * 64
-        ctx.render_device(sb, q, mimg.data_ptr())
-        acc += mimg
-    acc /= frames
-    rec["bsdf_only_4096spp_rel_rmse"] = _rel_rmse(acc, mref)
+    bimg, bnoise, _ = _reference_image(ctx, sb, sm_st, mwin)
+    rec["bsdf_only_4096spp_rel_rmse"] = float(np.sqrt(((bimg - mref) ** 2).mean()) / mref.mean())
+    rec["bsdf_only_4096spp_own_noise"] = bnoise
     ctx.free(sb)
     ctx.free(sm)
     out["mesh_box"] = rec

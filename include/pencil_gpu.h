@@ -349,10 +349,10 @@ typedef struct pgpu_scene_info {
                                   from pinned host memory by the upload      */
     int32_t n_leaves;          /* primitives (one per BVH leaf)              */
     int32_t n_interior;        /* interior nodes of the binary tree          */
-    int32_t n_wide;            /* 4-wide nodes collapsed from it             */
+    int32_t n_wide;            /* wide nodes collapsed from it               */
     int32_t bvh_depth;         /* levels of the binary tree                  */
     int32_t wide_stack;        /* traversal stack entries the wide tree needs */
-    int32_t reserved;
+    int32_t wide_width;        /* children per wide node (4 or 8)            */
 } pgpu_scene_info;
 int32_t pgpu_get_scene_info(pgpu_ctx* ctx, int32_t scene_id, pgpu_scene_info* out);
 

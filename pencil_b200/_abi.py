@@ -103,7 +103,7 @@ class Stats(C.Structure):
 class SceneInfo(C.Structure):
     _fields_ = [("device_bytes", C.c_int64), ("n_leaves", C.c_int32),
                 ("n_interior", C.c_int32), ("n_wide", C.c_int32), ("bvh_depth", C.c_int32),
-                ("wide_stack", C.c_int32), ("reserved", C.c_int32)]
+                ("wide_stack", C.c_int32), ("wide_width", C.c_int32)]
 
 
 EXPORTS = {

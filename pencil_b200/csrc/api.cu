@@ -887,6 +887,7 @@ int32_t pgpu_get_scene_info(pgpu_ctx* c, int32_t id, pgpu_scene_info* out) {
     info.n_wide = ds->n_wide;
     info.bvh_depth = ds->depth;
     info.wide_stack = ds->wide_stack;
+    info.wide_width = kWideWidth;
     *out = info;
     return PGPU_OK;
 }

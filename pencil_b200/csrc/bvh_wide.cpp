@@ -1,8 +1,9 @@
-// bvh_wide.cpp - 4-wide nodes collapsed from Pencil's binary tree.
+// bvh_wide.cpp - wide nodes collapsed from Pencil's binary tree.
 //
-// The wavefront kernels traverse a 4-wide tree made from the uploaded binary
-// tree (src/bvh.hpp:54-192 builds it): every wide node lists up to four
-// nodes of the binary tree as its children, with their boxes copied bit for
+// The kernels traverse a wide tree (kWideWidth children per node, 4 or 8)
+// made from the uploaded binary tree (src/bvh.hpp:54-192 builds it): every
+// wide node lists up to kWideWidth nodes of the binary tree as its children,
+// with their boxes copied bit for
 // bit. The boxes a ray is tested against are therefore Pencil's boxes; a
 // wide node only skips the boxes of the intermediate binary nodes, and since
 // a child's box lies inside its parent's and the slab test's rounding is
@@ -11,8 +12,9 @@
 //
 // Collapse: a wide node starts from the two children of a binary interior
 // node and repeatedly replaces its interior child of largest surface area by
-// that child's two children, keeping left-to-right order, until it has four
-// children or only leaves. Wide nodes are numbered in DFS pre-order.
+// that child's two children, keeping left-to-right order, until it has
+// kWideWidth children or only leaves. Wide nodes are numbered in DFS
+// pre-order.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -31,16 +33,45 @@ float area(const pgpu_bvh_node& n) {
     return 2.0f * (dx * dy + dy * dz + dz * dx);
 }
 
-void write_node(float4* q, const float (&lo)[3][4], const float (&hi)[3][4], const int (&ref)[4]) {
-    q[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
-    q[1] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
-    q[2] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
-    q[3] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
-    q[4] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
-    q[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
-    static_assert(sizeof(ref) == sizeof(float4), "four refs fill one float4");
-    std::memcpy(&q[6], ref, sizeof(ref));
-    q[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+constexpr int W = kWideWidth;
+constexpr int G = kWideGroups;
+
+// The node's rows (scene_layout.h): per axis the lo planes of children
+// 4g..4g+3 at row a*G + g, the hi planes at (3 + a)*G + g, refs at 6G + g.
+void write_node(float4* q, const float (&lo)[3][W], const float (&hi)[3][W], const int (&ref)[W]) {
+    for (int a = 0; a < 3; ++a)
+        for (int g = 0; g < G; ++g) {
+            const int k = 4 * g;
+            q[a * G + g] = make_float4(lo[a][k], lo[a][k + 1], lo[a][k + 2], lo[a][k + 3]);
+            q[(3 + a) * G + g] = make_float4(hi[a][k], hi[a][k + 1], hi[a][k + 2], hi[a][k + 3]);
+        }
+    static_assert(sizeof(ref) == G * sizeof(float4), "the refs fill G float4");
+    std::memcpy(&q[6 * G], ref, sizeof(ref));
+    for (int r = 7 * G; r < 8 * G; ++r) q[r] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// Expands the children of a wide node rooted at binary interior node b:
+// the interior child of largest surface area is replaced by its two
+// children while there are fewer than `cap`; returns the child count.
+int expand(const pgpu_bvh_node* nodes, int b, int cap, int (&ch)[W]) {
+    ch[0] = nodes[b].left;
+    ch[1] = nodes[b].right;
+    int n = 2;
+    while (n < cap) {
+        int pick = -1;
+        float best = -1.0f;
+        for (int k = 0; k < n; ++k) {
+            const pgpu_bvh_node& c = nodes[ch[k]];
+            if (c.left >= 0 && area(c) > best) { best = area(c); pick = k; }
+        }
+        if (pick < 0) break;
+        const int l = nodes[ch[pick]].left, r = nodes[ch[pick]].right;
+        for (int k = n; k > pick + 1; --k) ch[k] = ch[k - 1];
+        ch[pick] = l;
+        ch[pick + 1] = r;
+        ++n;
+    }
+    return n;
 }
 
 // Copies each subtree's block into `out` at base[t], its interior refs
@@ -52,8 +83,8 @@ void parallel_relocate(float4* out, const std::vector<std::vector<float4>>& loca
         float4* dst = out + (size_t)base[t] * kWideNodeFloat4;
         std::copy_n(local[t].begin(), (size_t)cnt * kWideNodeFloat4, dst);
         for (int w = 0; w < cnt; ++w) {
-            int* refs = reinterpret_cast<int*>(dst + (size_t)w * kWideNodeFloat4 + 6);
-            for (int k = 0; k < 4; ++k)
+            int* refs = reinterpret_cast<int*>(dst + (size_t)w * kWideNodeFloat4 + 6 * G);
+            for (int k = 0; k < W; ++k)
                 if (refs[k] >= 0) refs[k] += base[t];
         }
     });
@@ -62,7 +93,7 @@ void parallel_relocate(float4* out, const std::vector<std::vector<float4>>& loca
 struct Collapser {
     const pgpu_bvh_node* nodes;
     const std::vector<int>& leaf_ref;
-    bool expand;
+    int cap;                 // children per node in this collapse
     std::vector<float4>& out;
     int n_wide = 0;
 
@@ -72,26 +103,12 @@ struct Collapser {
         const int w = n_wide++;
         if (out.size() < (size_t)n_wide * kWideNodeFloat4)
             out.resize(std::max(out.size() * 2, (size_t)n_wide * kWideNodeFloat4));
-        int ch[4] = {nodes[b].left, nodes[b].right, -1, -1};
-        int n = 2;
-        while (expand && n < 4) {
-            int pick = -1;
-            float best = -1.0f;
-            for (int k = 0; k < n; ++k) {
-                const pgpu_bvh_node& c = nodes[ch[k]];
-                if (c.left >= 0 && area(c) > best) { best = area(c); pick = k; }
-            }
-            if (pick < 0) break;
-            const int l = nodes[ch[pick]].left, r = nodes[ch[pick]].right;
-            for (int k = n; k > pick + 1; --k) ch[k] = ch[k - 1];
-            ch[pick] = l;
-            ch[pick + 1] = r;
-            ++n;
-        }
-        float lo[3][4], hi[3][4];
-        int ref[4];
+        int ch[W];
+        const int n = expand(nodes, b, cap, ch);
+        float lo[3][W], hi[3][W];
+        int ref[W];
         int interior = 0, deepest = 0;
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < W; ++k) {
             if (k >= n) {
                 // missing child: a box no finite ray enters and a leaf of no type
                 for (int a = 0; a < 3; ++a) { lo[a][k] = INFINITY; hi[a][k] = -INFINITY; }
@@ -122,7 +139,7 @@ struct Collapser {
 // kernels only follow refs), so the top comes first and each subtree's nodes
 // follow as one block in DFS pre-order.
 int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_ref,
-                      bool expand, int threads, float4* out, WideScratch& scratch,
+                      int cap, int threads, float4* out, WideScratch& scratch,
                       int& stack_need) {
     const int T = threads;
     // top: breadth-first over wide-node roots until enough subtrees wait
@@ -136,28 +153,14 @@ int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_r
     while (head < todo.size() && todo.size() - head < want) {
         const Pending p = todo[head++];
         // collapse one node without recursing into interior children
-        int ch[4] = {nodes[p.binary].left, nodes[p.binary].right, -1, -1};
-        int n = 2;
-        while (expand && n < 4) {
-            int pick = -1;
-            float best = -1.0f;
-            for (int k = 0; k < n; ++k) {
-                const pgpu_bvh_node& c = nodes[ch[k]];
-                if (c.left >= 0 && area(c) > best) { best = area(c); pick = k; }
-            }
-            if (pick < 0) break;
-            const int l = nodes[ch[pick]].left, r = nodes[ch[pick]].right;
-            for (int k = n; k > pick + 1; --k) ch[k] = ch[k - 1];
-            ch[pick] = l;
-            ch[pick + 1] = r;
-            ++n;
-        }
+        int ch[W];
+        const int n = expand(nodes, p.binary, cap, ch);
         const int w = n_top++;
         top.resize((size_t)n_top * kWideNodeFloat4);
         top_kids.emplace_back();
-        float lo[3][4], hi[3][4];
-        int ref[4];
-        for (int k = 0; k < 4; ++k) {
+        float lo[3][W], hi[3][W];
+        int ref[W];
+        for (int k = 0; k < W; ++k) {
             if (k >= n) {
                 for (int a = 0; a < 3; ++a) { lo[a][k] = INFINITY; hi[a][k] = -INFINITY; }
                 ref[k] = ~(kLeafNone << kLeafTypeShift);
@@ -181,7 +184,7 @@ int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_r
     if ((int)local.size() < n_tasks) local.resize(n_tasks);
     std::vector<int> local_n(n_tasks, 0), local_need(n_tasks, 0);
     auto run = [&](int t) {
-        Collapser c{nodes, leaf_ref, expand, local[t]};
+        Collapser c{nodes, leaf_ref, cap, local[t]};
         c.build(todo[head + t].binary, local_need[t]);
         local_n[t] = c.n_wide;
     };
@@ -202,7 +205,7 @@ int collapse_parallel(const pgpu_bvh_node* nodes, const std::vector<int>& leaf_r
     for (int t = 0; t < n_tasks; ++t) wide_of_todo[head + t] = base[t];
     for (size_t k = 1; k < todo.size(); ++k) {
         const Pending& p = todo[k];
-        int* refs = reinterpret_cast<int*>(out + (size_t)p.parent * kWideNodeFloat4 + 6);
+        int* refs = reinterpret_cast<int*>(out + (size_t)p.parent * kWideNodeFloat4 + 6 * G);
         refs[p.child] = wide_of_todo[k];
     }
     parallel_relocate(out, local, local_n, base);
@@ -228,12 +231,14 @@ int collapse_wide(const pgpu_bvh_node* nodes, int n_nodes, const std::vector<int
     // a full binary tree of n_nodes nodes has (n_nodes - 1) / 2 interior ones
     const int n_interior = (n_nodes - 1) / 2;
     // greedy collapse; if a pathological tree would need a deeper stack than
-    // the kernels hold, two children per node (the binary tree's own bound)
-    // threads only pay off for large trees
+    // the kernels hold, fewer children per node: 4, then two (the binary
+    // tree's own bound). Threads only pay off for large trees.
     const int threads = n_interior < 16384 ? 1 : host_threads();
     int n_wide = 0;
-    for (int pass = 0; pass < 2; ++pass) {
-        n_wide = collapse_parallel(nodes, leaf_ref, pass == 0, threads, out, scratch, stack_need);
+    const int caps[3] = {W, 4, 2};
+    for (int pass = 0; pass < 3; ++pass) {
+        if (pass > 0 && caps[pass] >= caps[pass - 1]) continue;
+        n_wide = collapse_parallel(nodes, leaf_ref, caps[pass], threads, out, scratch, stack_need);
         if (stack_need <= max_stack) break;
     }
     return n_wide;

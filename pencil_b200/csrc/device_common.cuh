@@ -123,7 +123,7 @@ __device__ __forceinline__ void sample_uv(int i, int j, int sx, int sy, int W, i
 struct RayPre {
     V3 o, inv;
     bool nx, ny, nz;  // inv < 0: near plane is the box max
-    int ox, oy, oz;   // 4-wide nodes: float4 offset of the near planes (0: lo, 3: hi)
+    int ox, oy, oz;   // wide nodes: row of the near planes (0: lo, 3: hi), times G
 };
 __device__ __forceinline__ RayPre prep(const Ray& r) {
     RayPre p;
@@ -659,25 +659,35 @@ struct AnyTrav {
     }
 };
 
-// ---- 4-wide traversal (wavefront) ------------------------------------------------
-// One wide node as one ray sees it: its four child boxes' near and far
-// planes per axis (SoA float4 each) and refs. A node stores the lo planes of
+// ---- wide traversal (both engines) ---------------------------------------------
+// One wide node as one ray sees it: its children's near and far planes per
+// axis (rows of four, SoA float4) and refs. A node stores the lo planes of
 // x, y, z, then the hi planes; the ray's octant picks which are near, so the
 // loads, not per-child selects, put the planes in slab order.
+// A 4-wide node is held whole (six plane rows and the refs); an 8-wide node
+// keeps its refs and its address, and its plane rows are loaded a group of
+// four children at a time by slab_wide (a whole 8-wide node would take 56
+// registers).
 struct WideNode {
-    float4 nr[3], fr[3];
-    int4 ref;
+    float4 nr[3][1], fr[3][1];   // 4-wide: the plane rows (unused when 8-wide)
+    const float4* np;
+    int4 ref[kWideGroups];
 };
 __device__ __forceinline__ WideNode load_wide(const float4* wide, int node, const RayPre& r) {
     const float4* np = wide + (size_t)kWideNodeFloat4 * node;
+    constexpr int G = kWideGroups;
     WideNode w;
-    w.nr[0] = __ldg(np + r.ox);
-    w.fr[0] = __ldg(np + 3 - r.ox);
-    w.nr[1] = __ldg(np + 1 + r.oy);
-    w.fr[1] = __ldg(np + 4 - r.oy);
-    w.nr[2] = __ldg(np + 2 + r.oz);
-    w.fr[2] = __ldg(np + 5 - r.oz);
-    w.ref = __ldg(reinterpret_cast<const int4*>(np + 6));
+    w.np = np;
+    if constexpr (kWideWidth == 4) {
+        w.nr[0][0] = __ldg(np + r.ox);
+        w.fr[0][0] = __ldg(np + 3 - r.ox);
+        w.nr[1][0] = __ldg(np + 1 + r.oy);
+        w.fr[1][0] = __ldg(np + 4 - r.oy);
+        w.nr[2][0] = __ldg(np + 2 + r.oz);
+        w.fr[2][0] = __ldg(np + 5 - r.oz);
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) w.ref[g] = __ldg(reinterpret_cast<const int4*>(np + 6 * G + g));
     return w;
 }
 
@@ -698,32 +708,76 @@ __device__ __forceinline__ bool slab_nf(float nx, float ny, float nz, float fx, 
     return !(ex < en);
 }
 
-// Slab tests of the four children: bit k of the result is child k's hit,
-// e[k] its entry distance.
-__device__ __forceinline__ unsigned slab4(const WideNode& w, const RayPre& r, float tmin,
-                                          float tmax, float (&e)[4]) {
+__device__ __forceinline__ float f4c(const float4& v, int c) {
+    return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ int i4c(const int4& v, int c) {
+    return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+}
+
+// Slab tests of every child: bit k of the result is child k's hit, e[k] its
+// entry distance.
+__device__ __forceinline__ unsigned slab_wide(const WideNode& w, const RayPre& r, float tmin,
+                                              float tmax, float (&e)[kWideWidth]) {
     unsigned m = 0;
-    m |= slab_nf(w.nr[0].x, w.nr[1].x, w.nr[2].x, w.fr[0].x, w.fr[1].x, w.fr[2].x, r, tmin,
-                 tmax, e[0]) ? 1u : 0u;
-    m |= slab_nf(w.nr[0].y, w.nr[1].y, w.nr[2].y, w.fr[0].y, w.fr[1].y, w.fr[2].y, r, tmin,
-                 tmax, e[1]) ? 2u : 0u;
-    m |= slab_nf(w.nr[0].z, w.nr[1].z, w.nr[2].z, w.fr[0].z, w.fr[1].z, w.fr[2].z, r, tmin,
-                 tmax, e[2]) ? 4u : 0u;
-    m |= slab_nf(w.nr[0].w, w.nr[1].w, w.nr[2].w, w.fr[0].w, w.fr[1].w, w.fr[2].w, r, tmin,
-                 tmax, e[3]) ? 8u : 0u;
-    return m;
+    if constexpr (kWideWidth == 4) {
+        m |= slab_nf(w.nr[0][0].x, w.nr[1][0].x, w.nr[2][0].x, w.fr[0][0].x, w.fr[1][0].x,
+                     w.fr[2][0].x, r, tmin, tmax, e[0]) ? 1u : 0u;
+        m |= slab_nf(w.nr[0][0].y, w.nr[1][0].y, w.nr[2][0].y, w.fr[0][0].y, w.fr[1][0].y,
+                     w.fr[2][0].y, r, tmin, tmax, e[1]) ? 2u : 0u;
+        m |= slab_nf(w.nr[0][0].z, w.nr[1][0].z, w.nr[2][0].z, w.fr[0][0].z, w.fr[1][0].z,
+                     w.fr[2][0].z, r, tmin, tmax, e[2]) ? 4u : 0u;
+        m |= slab_nf(w.nr[0][0].w, w.nr[1][0].w, w.nr[2][0].w, w.fr[0][0].w, w.fr[1][0].w,
+                     w.fr[2][0].w, r, tmin, tmax, e[3]) ? 8u : 0u;
+        return m;
+    }
+    else {
+        constexpr int G = kWideGroups;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const float4 n0 = __ldg(w.np + r.ox * G + g), f0 = __ldg(w.np + (3 - r.ox) * G + g);
+            const float4 n1 = __ldg(w.np + (1 + r.oy) * G + g);
+            const float4 f1 = __ldg(w.np + (4 - r.oy) * G + g);
+            const float4 n2 = __ldg(w.np + (2 + r.oz) * G + g);
+            const float4 f2 = __ldg(w.np + (5 - r.oz) * G + g);
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                m |= slab_nf(f4c(n0, c), f4c(n1, c), f4c(n2, c), f4c(f0, c), f4c(f1, c),
+                             f4c(f2, c), r, tmin, tmax, e[4 * g + c]) ? (1u << (4 * g + c)) : 0u;
+        }
+        return m;
+    }
 }
 
 // Child k's ref / entry distance by a select chain (no local-memory indexing).
-__device__ __forceinline__ int pick_ref(const int4& r, int k) {
-    return k == 0 ? r.x : k == 1 ? r.y : k == 2 ? r.z : r.w;
+__device__ __forceinline__ int pick_ref(const WideNode& w, int k) {
+    if constexpr (kWideWidth == 4) {
+        const int4& r = w.ref[0];
+        return k == 0 ? r.x : k == 1 ? r.y : k == 2 ? r.z : r.w;
+    }
+    int v = w.ref[0].x;
+#pragma unroll
+    for (int j = 1; j < kWideWidth; ++j) v = k == j ? i4c(w.ref[j >> 2], j & 3) : v;
+    return v;
 }
-__device__ __forceinline__ float pick_e(const float (&e)[4], int k) {
-    return k == 0 ? e[0] : k == 1 ? e[1] : k == 2 ? e[2] : e[3];
+__device__ __forceinline__ float pick_e(const float (&e)[kWideWidth], int k) {
+    if constexpr (kWideWidth == 4) return k == 0 ? e[0] : k == 1 ? e[1] : k == 2 ? e[2] : e[3];
+    float v = e[0];
+#pragma unroll
+    for (int j = 1; j < kWideWidth; ++j) v = k == j ? e[j] : v;
+    return v;
 }
 // Children of a wide node whose ref is a leaf, as bits.
-__device__ __forceinline__ unsigned leaf_bits(const int4& r) {
-    return (r.x < 0 ? 1u : 0u) | (r.y < 0 ? 2u : 0u) | (r.z < 0 ? 4u : 0u) | (r.w < 0 ? 8u : 0u);
+__device__ __forceinline__ unsigned leaf_bits(const WideNode& w) {
+    if constexpr (kWideWidth == 4) {
+        const int4& r = w.ref[0];
+        return (r.x < 0 ? 1u : 0u) | (r.y < 0 ? 2u : 0u) | (r.z < 0 ? 4u : 0u) |
+               (r.w < 0 ? 8u : 0u);
+    }
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < kWideWidth; ++k) m |= i4c(w.ref[k >> 2], k & 3) < 0 ? (1u << k) : 0u;
+    return m;
 }
 
 // Sorts four (key, ref) pairs by key, ascending (a five-exchange network).
@@ -745,7 +799,54 @@ __device__ __forceinline__ void sort4(float& k0, int& r0, float& k1, int& r1, fl
     cs(k1, r1, k2, r2);
 }
 
-// Resumable closest-hit traversal of the 4-wide tree. Same result rule as
+// The interior children of mask `im` with entries e: all but the nearest
+// stacked, farthest first (so they pop nearest first); returns the nearest.
+// 4-wide nodes sort their four keys with a network; 8-wide nodes take the
+// farthest remaining child at each push.
+template <int kShared>
+__device__ __forceinline__ int push_children(const WideNode& w, unsigned im,
+                                             const float (&e)[kWideWidth],
+                                             TravStack<kShared>& stk, int& sp, bool keyed) {
+    if constexpr (kWideWidth == 4) {
+        float k0 = (im & 1u) ? e[0] : INFINITY;
+        float k1 = (im & 2u) ? e[1] : INFINITY;
+        float k2 = (im & 4u) ? e[2] : INFINITY;
+        float k3 = (im & 8u) ? e[3] : INFINITY;
+        int r0 = w.ref[0].x, r1 = w.ref[0].y, r2 = w.ref[0].z, r3 = w.ref[0].w;
+        sort4(k0, r0, k1, r1, k2, r2, k3, r3);
+        if (k3 != INFINITY) stk.push(sp++, r3, keyed ? k3 : 0.0f);
+        if (k2 != INFINITY) stk.push(sp++, r2, keyed ? k2 : 0.0f);
+        if (k1 != INFINITY) stk.push(sp++, r1, keyed ? k1 : 0.0f);
+        return r0;
+    } else if (!keyed) {
+        // any hit: the nearest child next, the others in child order
+        int kn = __ffs(im) - 1;
+        float en = INFINITY;
+#pragma unroll
+        for (int k = 0; k < kWideWidth; ++k)
+            if (((im >> k) & 1u) && e[k] < en) { en = e[k]; kn = k; }
+        im &= ~(1u << kn);
+        while (im) {
+            const int k = 31 - __clz(im);
+            im &= ~(1u << k);
+            stk.push(sp++, pick_ref(w, k), 0.0f);
+        }
+        return pick_ref(w, kn);
+    } else {
+        while (__popc(im) > 1) {
+            int kf = 0;
+            float ef = -INFINITY;
+#pragma unroll
+            for (int k = 0; k < kWideWidth; ++k)
+                if (((im >> k) & 1u) && e[k] >= ef) { ef = e[k]; kf = k; }
+            stk.push(sp++, pick_ref(w, kf), keyed ? ef : 0.0f);
+            im &= ~(1u << kf);
+        }
+        return pick_ref(w, __ffs(im) - 1);
+    }
+}
+
+// Resumable closest-hit traversal of the wide tree. Same result rule as
 // ClosestTrav (smallest t, ties to the later DFS leaf); children are taken
 // nearest first, the others stacked with their entry distance.
 template <int kShared, bool COUNT>
@@ -791,27 +892,22 @@ struct ClosestTrav4 {
                                          TravCount* cnt) {
         const WideNode w = load_wide(S.wide, node, rp);
         if (COUNT) cnt->nodes++;
-        float e[4];
-        unsigned m = slab4(w, rp, tmin, t_best, e);
-        unsigned lm = m & leaf_bits(w.ref);
+        float e[kWideWidth];
+        unsigned m = slab_wide(w, rp, tmin, t_best, e);
+        unsigned lm = m & leaf_bits(w);
         m &= ~lm;
         while (lm) {
             const int k = __ffs(lm) - 1;
             lm &= lm - 1;
-            if (pick_e(e, k) <= t_best) test_leaf(S, pick_ref(w.ref, k), cnt);
+            if (pick_e(e, k) <= t_best) test_leaf(S, pick_ref(w, k), cnt);
         }
-        // interior children still in reach, nearest first (sorting network)
-        float k0 = (m & 1u) && e[0] <= t_best ? e[0] : INFINITY;
-        float k1 = (m & 2u) && e[1] <= t_best ? e[1] : INFINITY;
-        float k2 = (m & 4u) && e[2] <= t_best ? e[2] : INFINITY;
-        float k3 = (m & 8u) && e[3] <= t_best ? e[3] : INFINITY;
-        int r0 = w.ref.x, r1 = w.ref.y, r2 = w.ref.z, r3 = w.ref.w;
-        sort4(k0, r0, k1, r1, k2, r2, k3, r3);
-        if (k0 != INFINITY) {
-            if (k3 != INFINITY) stk.push(sp++, r3, k3);
-            if (k2 != INFINITY) stk.push(sp++, r2, k2);
-            if (k1 != INFINITY) stk.push(sp++, r1, k1);
-            node = r0;
+        // interior children still in reach, nearest first
+        unsigned im = 0;
+#pragma unroll
+        for (int k = 0; k < kWideWidth; ++k)
+            if (((m >> k) & 1u) && e[k] <= t_best) im |= 1u << k;
+        if (im) {
+            node = push_children(w, im, e, stk, sp, true);
             return false;
         }
         while (sp > 0) {
@@ -825,7 +921,7 @@ struct ClosestTrav4 {
     }
 };
 
-// Resumable any-hit traversal of the 4-wide tree (BVHNode::occluded,
+// Resumable any-hit traversal of the wide tree (BVHNode::occluded,
 // src/bvh.hpp:39-48): with a fixed t_max the set of boxes entered does not
 // depend on the order, so the answer equals the reference's whatever order
 // the children are taken in.
@@ -868,28 +964,19 @@ struct AnyTrav4 {
                                          TravCount* cnt) {
         const WideNode w = load_wide(S.wide, node, rp);
         if (COUNT) cnt->nodes++;
-        float e[4];
-        unsigned m = slab4(w, rp, tmin, tmax, e);
-        unsigned lm = m & leaf_bits(w.ref);
+        float e[kWideWidth];
+        unsigned m = slab_wide(w, rp, tmin, tmax, e);
+        unsigned lm = m & leaf_bits(w);
         m &= ~lm;
         while (lm) {
             const int k = __ffs(lm) - 1;
             lm &= lm - 1;
-            if (test_leaf(S, pick_ref(w.ref, k), cnt)) { hit = true; return true; }
+            if (test_leaf(S, pick_ref(w, k), cnt)) { hit = true; return true; }
         }
         if (m) {
             // nearest child first, the others stacked so that the nearer pop
             // first: an occluder near the ray's origin ends the walk early
-            float k0 = (m & 1u) ? e[0] : INFINITY;
-            float k1 = (m & 2u) ? e[1] : INFINITY;
-            float k2 = (m & 4u) ? e[2] : INFINITY;
-            float k3 = (m & 8u) ? e[3] : INFINITY;
-            int r0 = w.ref.x, r1 = w.ref.y, r2 = w.ref.z, r3 = w.ref.w;
-            sort4(k0, r0, k1, r1, k2, r2, k3, r3);
-            if (k3 != INFINITY) stk.push(sp++, r3, 0.0f);
-            if (k2 != INFINITY) stk.push(sp++, r2, 0.0f);
-            if (k1 != INFINITY) stk.push(sp++, r1, 0.0f);
-            node = r0;
+            node = push_children(w, m, e, stk, sp, false);
             return false;
         }
         if (sp == 0) return true;

@@ -12,13 +12,17 @@
 //             [4i+2] = (R.min.z, R.max.x, R.max.y, R.max.z)
 //             [4i+3] = (ref L, ref R, -, -)            (int bits)
 //           ref >= 0: interior node index; ref < 0: leaf, ~ref = type<<28 | slot
-//   wide    float4[8 * n_wide]      4-wide nodes collapsed from the same tree
-//                                   (bvh_wide.cpp), used by the wavefront:
-//             [8i+0..2] = min.x, min.y, min.z of children 0..3
-//             [8i+3..5] = max.x, max.y, max.z of children 0..3
-//             [8i+6]    = refs of children 0..3 (int bits; a missing child
-//                         has an empty box and a leaf ref of type LEAF_NONE)
-//             [8i+7]    = unused
+//   wide    float4[kWideNodeFloat4 * n_wide]
+//                                   W-wide nodes (W = kWideWidth, 4 or 8)
+//                                   collapsed from the same tree
+//                                   (bvh_wide.cpp), used by both engines;
+//                                   with G = W / 4 float4 per row of W floats:
+//             [(a    )*G + g] = min of axis a (x, y, z) of children 4g..4g+3
+//             [(3 + a)*G + g] = max of axis a of the same children
+//             [6G + g]        = refs of those children (int bits; a missing
+//                               child has an empty box and a leaf ref of type
+//                               LEAF_NONE)
+//             [7G .. 8G)      = unused
 //   geo_a   float4[n_leaves]        leaf geometry in DFS leaf order (slot):
 //             sphere   (center.xyz, radius)
 //             triangle (v0.xyz, -)
@@ -62,7 +66,14 @@ enum LeafType : int {
     LEAF_NONE = 7,          // placeholder child of a wide node: never hit
 };
 constexpr int kLeafNone = LEAF_NONE;
-constexpr int kWideNodeFloat4 = 8;
+// Children per wide node, fixed at compile time (4 or 8).
+#ifndef PGPU_WIDE_WIDTH
+#define PGPU_WIDE_WIDTH 4
+#endif
+constexpr int kWideWidth = PGPU_WIDE_WIDTH;
+static_assert(kWideWidth == 4 || kWideWidth == 8, "wide nodes have 4 or 8 children");
+constexpr int kWideGroups = kWideWidth / 4;          // float4 per row of child planes
+constexpr int kWideNodeFloat4 = 8 * kWideGroups;     // 128 or 256 bytes
 
 constexpr int kLeafTypeShift = 28;
 constexpr int kLeafSlotMask = (1 << kLeafTypeShift) - 1;
@@ -96,7 +107,7 @@ struct alignas(16) DevLight {
 // single-scene launches and read from global memory for batched ones.
 struct SceneView {
     const float4* nodes;
-    const float4* wide;    // 4-wide nodes (null when the root is a leaf)
+    const float4* wide;    // wide nodes (null when the root is a leaf)
     const float4* geo_a;
     const float4* geo_b;
     const float4* geo_c;   // null in scenes without triangles

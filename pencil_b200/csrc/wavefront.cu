@@ -375,7 +375,7 @@ __device__ __forceinline__ void warp_append(bool take, int slot, int* counter, i
 // ---- extend, camera rays of one scene: warp packets ------------------------------
 // The first bounce's queue holds the camera rays in slot order, so a warp's
 // 32 rays are the samples of two neighbouring pixels: nearly the same ray.
-// The warp traverses the 4-wide tree once for all of them: every lane tests
+// The warp traverses the wide tree once for all of them: every lane tests
 // every node the packet enters against its own ray and its own t_best, the
 // packet enters a child that any lane still reaches (nearest first by the
 // lanes' smallest entry distance), and one shared stack serves the warp.
@@ -414,23 +414,32 @@ __global__ void __launch_bounds__(kWfMaxBlock) wf_extend_packet(WfArgs A) {
             while (true) {
                 const WideNode w = load_wide(S.wide, node, tr.rp);
                 if (COUNT && active) rc.tc.nodes++;
-                float ee[4];
-                unsigned m = active ? slab4(w, tr.rp, tr.tmin, tr.t_best, ee) : 0u;
-                const unsigned lm = m & leaf_bits(w.ref);
+                float ee[kWideWidth];
+                unsigned m = active ? slab_wide(w, tr.rp, tr.tmin, tr.t_best, ee) : 0u;
+                const unsigned lm = m & leaf_bits(w);
                 m &= ~lm;
                 unsigned ulm = __reduce_or_sync(0xffffffffu, lm);
                 while (ulm) {
                     const int k = __ffs(ulm) - 1;
                     ulm &= ulm - 1;
                     if (((lm >> k) & 1u) && pick_e(ee, k) <= tr.t_best)
-                        tr.test_leaf(S, pick_ref(w.ref, k), &rc.tc);
+                        tr.test_leaf(S, pick_ref(w, k), &rc.tc);
                 }
                 // per child, the smallest entry distance of a lane that still
                 // reaches it (entries are positive: their bits order as ints)
-                float key[4];
-                int ref[4] = {w.ref.x, w.ref.y, w.ref.z, w.ref.w};
+                float key[kWideWidth];
+                int ref[kWideWidth];
+                if constexpr (kWideWidth == 4) {
+                    ref[0] = w.ref[0].x;
+                    ref[1] = w.ref[0].y;
+                    ref[2] = w.ref[0].z;
+                    ref[3] = w.ref[0].w;
+                } else {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                    for (int k = 0; k < kWideWidth; ++k) ref[k] = i4c(w.ref[k >> 2], k & 3);
+                }
+#pragma unroll
+                for (int k = 0; k < kWideWidth; ++k) {
                     const bool reach = ((m >> k) & 1u) && ee[k] <= tr.t_best;
                     key[k] = __uint_as_float(__reduce_min_sync(
                         0xffffffffu, reach ? __float_as_uint(ee[k]) : 0x7f800000u));
@@ -440,18 +449,24 @@ __global__ void __launch_bounds__(kWfMaxBlock) wf_extend_packet(WfArgs A) {
                 int best = 0;
                 float kb = key[0];
 #pragma unroll
-                for (int k = 1; k < 4; ++k)
+                for (int k = 1; k < kWideWidth; ++k)
                     if (key[k] < kb) { kb = key[k]; best = k; }
                 if (kb != INFINITY) {
                     __syncwarp();
 #pragma unroll
-                    for (int k = 3; k >= 0; --k)
+                    for (int k = kWideWidth - 1; k >= 0; --k)
                         if (k != best && key[k] != INFINITY) {
                             if (lane == 0) { sref[sp] = ref[k]; skey[sp] = key[k]; }
                             ++sp;
                         }
                     __syncwarp();
-                    node = best == 0 ? ref[0] : best == 1 ? ref[1] : best == 2 ? ref[2] : ref[3];
+                    if constexpr (kWideWidth == 4) {
+                        node = best == 0 ? ref[0] : best == 1 ? ref[1] : best == 2 ? ref[2] : ref[3];
+                    } else {
+                        node = ref[0];
+#pragma unroll
+                        for (int k = 1; k < kWideWidth; ++k) node = best == k ? ref[k] : node;
+                    }
                     continue;
                 }
                 // pop the nearest entry some lane may still reach
@@ -700,8 +715,12 @@ wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
 // lane refill as extend. A lane owns one slot: it resolves the slot's records
 // in the order shade made them, feeding each visibility into the same
 // NeeAccum as the megakernel, then applies the pending terms to L.
+// 8-wide nodes: at most 85 registers (three blocks of 256 threads per SM);
+// left free the kernel takes 127 and fits too few warps to hide latency.
+constexpr int kShadowMinBlocks = kWideWidth == 8 ? 3 : 1;
+
 template <bool COUNT, bool ONE>
-__global__ void __launch_bounds__(kWfMaxBlock)
+__global__ void __launch_bounds__(kWfMaxBlock, kShadowMinBlocks)
 wf_shadow(WfArgs A, int it) {
     extern __shared__ int smem[];
     TravStack<kWfShared> stk;

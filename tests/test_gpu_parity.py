@@ -401,9 +401,11 @@ def test_scene_info_sizes(gpu, scenes):
         n = scene.n_unified
         assert info["n_leaves"] == n and info["n_interior"] == max(n - 1, 0)
         assert 0 < info["n_wide"] <= info["n_interior"] or n <= 1
-        assert info["n_wide"] >= (info["n_interior"] + 2) // 3
+        wd = info["wide_width"]
+        assert wd in (4, 8)
+        assert info["n_wide"] >= (info["n_interior"] + wd - 2) // (wd - 1)
         assert 0 <= info["wide_stack"] <= 64 and 1 <= info["bvh_depth"] <= 64
-        assert info["device_bytes"] >= info["n_interior"] * 64 + info["n_wide"] * 128 + n * 40
+        assert info["device_bytes"] >= info["n_interior"] * 64 + info["n_wide"] * 32 * wd + n * 40
 
 
 def test_invalid_arguments_return_status(gpu):
