@@ -715,9 +715,10 @@ wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
 // lane refill as extend. A lane owns one slot: it resolves the slot's records
 // in the order shade made them, feeding each visibility into the same
 // NeeAccum as the megakernel, then applies the pending terms to L.
-// 8-wide nodes: at most 85 registers (three blocks of 256 threads per SM);
-// left free the kernel takes 127 and fits too few warps to hide latency.
-constexpr int kShadowMinBlocks = kWideWidth == 8 ? 3 : 1;
+// At most 80 registers (three blocks of 256 or six of 128 threads per SM):
+// left free the kernel takes 105 (127 with 8-wide nodes), which leaves four
+// blocks of 128 per SM -- too few warps to hide the latency of its loads.
+constexpr int kShadowMinBlocks = 3;
 
 template <bool COUNT, bool ONE>
 __global__ void __launch_bounds__(kWfMaxBlock, kShadowMinBlocks)
