@@ -234,7 +234,8 @@ typedef struct pgpu_render_params {
     uint32_t seed;              /* salt mixed into the counter RNG (0: none) */
     int32_t  sample_offset;     /* first sample index (progressive renders)  */
     int32_t  flags;             /* enum pgpu_flags                           */
-    int32_t  queue_capacity;    /* wavefront paths in flight (0: automatic)  */
+    int32_t  queue_capacity;    /* wavefront paths in flight, 0..2^28 (0:
+                                   automatic)                                */
     int32_t  refill_below;      /* wavefront: a warp takes new rays once at
                                    most this many of its 32 lanes are still
                                    traversing (0: automatic)                 */

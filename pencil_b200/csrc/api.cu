@@ -999,6 +999,8 @@ int make_cfg(pgpu_ctx* c, const DeviceScene* ds, const pgpu_render_params* p, Re
     if (p->refill_below < 0 || p->refill_below > 31)
         return fail(c, PGPU_ERR_INVALID_ARG, "refill_below must be 0..31");
     cfg.refill = p->refill_below;
+    if (p->queue_capacity < 0 || p->queue_capacity > (1 << 28))
+        return fail(c, PGPU_ERR_INVALID_ARG, "queue_capacity must be 0..2^28 paths");
     cfg.queue_capacity = p->queue_capacity;
     if (p->sort_key < 0 || p->sort_key > 3)
         return fail(c, PGPU_ERR_INVALID_ARG, "sort_key must be 0..3");

@@ -609,7 +609,7 @@ wf_shade(WfArgs A, int it) {
             first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
             if (alive && bin == b) {
                 const int pos = first + __popc(m & ((1u << lane) - 1u));
-                qout[b * A.Q + pos] = slot;
+                qout[(size_t)b * A.Q + pos] = slot;
                 if (A.sort_key == 3) A.key_e[pos] = key_next;   // one bin under key 3
             }
         }
