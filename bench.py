@@ -675,8 +675,11 @@ def measure_quality(ctx, sid, st, stream) -> dict:
 
 
 def measure_bvh_build(ctx, stream) -> dict:
-    """Pencil's host SAH build against the device LBVH build, and the render
-    time on each tree (sphere cloud, tuned launch parameters)."""
+    """Pencil's host SAH build against the device builds -- Pencil's binned
+    SAH (the same tree) and an LBVH -- and the render time on each tree
+    (wall-clock medians of 5 calls after a first one; the render on the
+    sphere cloud with the tuned launch parameters, on the mesh with its
+    autotuned ones)."""
     import time
 
     import torch
@@ -687,26 +690,32 @@ def measure_bvh_build(ctx, stream) -> dict:
         t0 = time.perf_counter()
         host_nodes, host_depth = wl.scene.build_bvh()
         host_ms = (time.perf_counter() - t0) * 1e3
-        ctx.build_bvh_device(wl.scene)                      # first call loads the module
-        times = []
-        for _ in range(5):                                  # median of 5 wall-clock calls
-            t0 = time.perf_counter()
-            dev_nodes, dev_depth = ctx.build_bvh_device(wl.scene)
-            times.append((time.perf_counter() - t0) * 1e3)
-        dev_ms = sorted(times)[2]
-        rec = {"primitives": wl.scene.n_unified, "host_sah_ms": host_ms, "host_depth": host_depth,
-               "device_lbvh_ms": dev_ms, "device_depth": dev_depth}
+        rec = {"primitives": wl.scene.n_unified, "host_sah_ms": host_ms, "host_depth": host_depth}
+        trees = {"sah": host_nodes}
+        for method in ("sah", "lbvh"):
+            ctx.build_bvh_device(wl.scene, method=method)   # first call loads the module
+            times = []
+            for _ in range(5):
+                t0 = time.perf_counter()
+                dev_nodes, dev_depth = ctx.build_bvh_device(wl.scene, method=method)
+                times.append((time.perf_counter() - t0) * 1e3)
+            rec[f"device_{method}_ms"] = sorted(times)[2]
+            rec[f"device_{method}_depth"] = dev_depth
+            trees[f"device_{method}"] = dev_nodes
+        rec["device_sah_same_nodes"] = float(np.mean(trees["device_sah"] == host_nodes))
+        st = wl.settings
+        st.engine = A.ENGINE_WAVEFRONT
         if name == "sphere_cloud":
-            st = wl.settings
-            st.engine = A.ENGINE_WAVEFRONT
             st.queue_capacity = st.width * st.height * st.samples ** 2
-            st.refill_below, st.sort_key = 16, 2
-            buf = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")
-            for tree, nodes in (("sah", host_nodes), ("lbvh", dev_nodes)):
-                sid = ctx.upload(wl.scene, nodes)
-                rec[f"render_ms_{tree}"] = _event_ms(
-                    stream, lambda: ctx.render_device(sid, st, buf.data_ptr()), 3)
-                ctx.free(sid)
+            st.refill_below, st.sort_key = 16, 3
+        else:
+            st.queue_capacity, st.refill_below, st.sort_key = 1 << 26, 16, 3
+        buf = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")
+        for tree, nodes in trees.items():
+            sid = ctx.upload(wl.scene, nodes)
+            rec[f"render_ms_{tree}"] = _event_ms(
+                stream, lambda: ctx.render_device(sid, st, buf.data_ptr()), 2)
+            ctx.free(sid)
         out[name] = rec
     return out
 
@@ -730,8 +739,8 @@ def measure_mesh(ctx, stream) -> dict:
     info = ctx.scene_info(sm)
     st = wm.settings
     paths = st.width * st.height * st.samples ** 2
-    # launch parameters for this workload from the autotuner (its capacity
-    # candidates stop at 16M paths, several chunks of this frame)
+    # launch parameters for this workload from the autotuner (capacity
+    # candidates up to 2^26 paths: the whole frame in one chunk)
     from pencil_b200.autotune import autotune
     tuned = autotune(ctx, [sm], [st], scene=wm.scene, reps=1, use_cache=False)
     buf = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")

@@ -4,7 +4,10 @@ The wavefront renderer has four knobs whose best values depend on the
 workload (image size, samples, scene, light count) and the GPU:
 
   queue_capacity  paths in flight per chunk: more paths keep late bounces
-                  busy but cost scratch memory (about 256 B per path)
+                  busy but cost scratch memory (about 212 B per path plus
+                  64 B per shadow record a vertex can make); candidates
+                  from 2^20 to 2^26 paths, as far as half the free device
+                  memory holds them
   refill_below    a warp of the persistent traversal kernels fetches new rays
                   once at most this many of its lanes are still traversing
   sort_key        0: queue order; 1: rays binned by direction octant;
@@ -35,7 +38,10 @@ from .renderer import GpuContext, RenderSettings
 CACHE = Path(os.environ.get("PGPU_AUTOTUNE_CACHE",
                             Path.home() / ".cache" / "pencil_b200" / "autotune.json"))
 
-CAPACITIES = (1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24)
+CAPACITIES = (1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26)
+# scratch per path in flight, bounded above: path state 128 B, queues 64 B,
+# sort lists 20 B and up to four 64-byte shadow records
+SCRATCH_BYTES_PER_PATH = 512
 REFILLS = (12, 16, 20, 24)
 SORT_KEYS = (0, 1, 2, 3)
 BLOCKS = (64, 128, 256)
@@ -113,7 +119,10 @@ def autotune(ctx: GpuContext, sids: list[int], settings: list[RenderSettings], s
             log(f"autotune q={q} refill={r} sort={s} block={b}: {ms:.2f} ms")
         return ms
 
-    caps = [q for q in CAPACITIES if q < total_paths] + [min(total_paths, CAPACITIES[-1])]
+    # capacities whose scratch fits in half the free device memory
+    room = torch.cuda.mem_get_info()[0] // 2 // SCRATCH_BYTES_PER_PATH
+    fit = [q for q in CAPACITIES if q <= room] or [CAPACITIES[0]]
+    caps = [q for q in fit if q < total_paths] + [min(total_paths, fit[-1])]
     caps = sorted(set(caps))
     q_best = min(caps, key=lambda q: trial(q, 20, 0, 128))
     r_best = min(REFILLS, key=lambda r: trial(q_best, r, 0, 128))

@@ -48,10 +48,10 @@ int adjoint_max_lights();
 cudaError_t launch_tonemap(const float* d_hdr, long long n_pixels, int mode, float exposure,
                            uint8_t* d_out, const float* d_thr, cudaStream_t st);
 const float* gamma_thresholds_host();
-cudaError_t device_sah(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_node>& out,
-                       int& depth, cudaStream_t st);
-cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_node>& out,
-                        int& depth, cudaStream_t st);
+cudaError_t device_sah(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, int& depth,
+                       cudaStream_t st, cudaMemPool_t pool);
+cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, int& depth,
+                        cudaStream_t st, cudaMemPool_t pool);
 
 constexpr int kMaxDepth = 64;          // traversal stack bound (kMaxStack)
 constexpr int kMaxTreeFrames = 32;     // Whitted recursion bound of the two-branch mode
@@ -244,8 +244,9 @@ int first_bad(int n, P bad) {
     return first.load() < n ? first.load() : -1;
 }
 
-// Scene arena from the context's memory pool (created on first use).
-cudaError_t arena_alloc(pgpu_ctx* c, size_t bytes, void** out) {
+// The context's stream-ordered memory pool (created on first use): scene
+// arenas and device BVH builds allocate from it.
+cudaError_t ensure_pool(pgpu_ctx* c) {
     if (!c->pool) {
         cudaMemPoolProps props{};
         props.allocType = cudaMemAllocationTypePinned;
@@ -257,6 +258,13 @@ cudaError_t arena_alloc(pgpu_ctx* c, size_t bytes, void** out) {
         unsigned long long keep = ~0ull;
         cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
+    return cudaSuccess;
+}
+
+// Scene arena from the context's memory pool.
+cudaError_t arena_alloc(pgpu_ctx* c, size_t bytes, void** out) {
+    cudaError_t e = ensure_pool(c);
+    if (e != cudaSuccess) return e;
     return cudaMallocFromPoolAsync(out, bytes, c->pool, c->stream);
 }
 
@@ -504,12 +512,11 @@ static int32_t build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node*
         return PGPU_OK;
     }
     PGPU_CUDA(c, cudaSetDevice(c->device));
-    std::vector<pgpu_bvh_node> nodes;
+    PGPU_CUDA(c, ensure_pool(c));
     int depth = 0;
-    cudaError_t e = sah ? device_sah(*s, n, nodes, depth, c->stream)
-                        : device_lbvh(*s, n, nodes, depth, c->stream);
+    cudaError_t e = sah ? device_sah(*s, n, out_nodes, depth, c->stream, c->pool)
+                        : device_lbvh(*s, n, out_nodes, depth, c->stream, c->pool);
     if (e != cudaSuccess) return cuda_fail(c, e, "device BVH build");
-    std::memcpy(out_nodes, nodes.data(), nodes.size() * sizeof(pgpu_bvh_node));
     if (out_depth) *out_depth = depth;
     return PGPU_OK;
 }

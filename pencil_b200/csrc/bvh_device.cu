@@ -270,9 +270,17 @@ __global__ void lb_write(const unsigned long long* keys, int n, const int* left,
     }
 }
 
+// Build memory from the context's stream-ordered pool, returned to it on
+// the build's stream when the build ends (no device-wide synchronisation,
+// and a repeated build reuses the pool's memory).
 struct DevBuf {
     void* p = nullptr;
-    ~DevBuf() { if (p) cudaFree(p); }
+    cudaStream_t st = nullptr;
+    cudaError_t alloc(size_t bytes, cudaMemPool_t pool, cudaStream_t s) {
+        st = s;
+        return cudaMallocFromPoolAsync(&p, bytes, pool, s);
+    }
+    ~DevBuf() { if (p) cudaFreeAsync(p, st); }
 };
 
 // ---- binned SAH on the device ------------------------------------------------------
@@ -749,8 +757,8 @@ __global__ void sah_root(const int* bounds, int n, SahTask* tasks, SahSmall* sma
 
 // Builds the table on the current device; n_unified >= 2. Device memory for
 // the build is allocated here and freed before returning.
-cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_node>& out,
-                        int& depth, cudaStream_t st) {
+cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, int& depth,
+                        cudaStream_t st, cudaMemPool_t pool) {
     const int n = n_unified;
     const size_t np = (size_t)s.n_prims, nv = (size_t)s.n_mesh_vertices,
                  nt = (size_t)s.n_mesh_triangles;
@@ -766,7 +774,7 @@ cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh
                                    (unsigned long long*)nullptr, n, 0, 64, st);
     bytes += al(sort_bytes);
     DevBuf mem;
-    cudaError_t e = cudaMalloc(&mem.p, bytes);
+    cudaError_t e = mem.alloc(bytes, pool, st);
     if (e != cudaSuccess) return e;
     unsigned char* p = static_cast<unsigned char*>(mem.p);
     auto take = [&](size_t b) { unsigned char* r = p; p += al(b); return r; };
@@ -815,8 +823,7 @@ cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh
                                        d_pre, d_level, d_maxlvl);
     lb_write<<<grid(total), B, 0, st>>>(d_sorted, n, d_left, d_right, d_nbox, d_pre, d_out);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    out.resize(total);
-    if ((e = cudaMemcpyAsync(out.data(), d_out, total * sizeof(pgpu_bvh_node),
+    if ((e = cudaMemcpyAsync(out, d_out, total * sizeof(pgpu_bvh_node),
                              cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return e;
     if ((e = cudaMemcpyAsync(&depth, d_maxlvl, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
@@ -826,8 +833,8 @@ cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh
 
 // Pencil's binned SAH tree, built on the current device; n_unified >= 2.
 // Device memory for the build is allocated here and freed before returning.
-cudaError_t device_sah(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_node>& out,
-                       int& depth, cudaStream_t st) {
+cudaError_t device_sah(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, int& depth,
+                       cudaStream_t st, cudaMemPool_t pool) {
     const int n = n_unified;
     const size_t np = (size_t)s.n_prims, nv = (size_t)s.n_mesh_vertices,
                  nt = (size_t)s.n_mesh_triangles;
@@ -852,7 +859,7 @@ cudaError_t device_sah(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_
                    2 * al((size_t)n * 4) + 2 * al((size_t)n * 4) +
                    al(total * sizeof(pgpu_bvh_node)) + al(scan_bytes) + al(seg_bytes) + al(2 * 4);
     DevBuf mem;
-    cudaError_t e = cudaMalloc(&mem.p, bytes);
+    cudaError_t e = mem.alloc(bytes, pool, st);
     if (e != cudaSuccess) return e;
     unsigned char* p = static_cast<unsigned char*>(mem.p);
     auto take = [&](size_t b) { unsigned char* r = p; p += al(b); return r; };
@@ -981,8 +988,7 @@ cudaError_t device_sah(const pgpu_scene& s, int n_unified, std::vector<pgpu_bvh_
         sah_small<<<grid(host_ctr[0]), B, 0, st>>>(d_small, host_ctr[0], d_perm, d_boxes, d_out,
                                                   (int)total, d_misc + 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    out.resize(total);
-    if ((e = cudaMemcpyAsync(out.data(), d_out, total * sizeof(pgpu_bvh_node),
+    if ((e = cudaMemcpyAsync(out, d_out, total * sizeof(pgpu_bvh_node),
                              cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return e;
     if ((e = cudaMemcpyAsync(&depth, d_misc + 1, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
