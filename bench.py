@@ -460,6 +460,10 @@ def run_ours(args) -> None:
                                       else "1 GPU"},
             "mrays_per_s": mrays,
             "rays_per_step": rays,
+            # Pencil's own count (RenderStats::rays_traced: one per trace /
+            # trace_path call), for comparison with the reference's figures
+            "reference_rays_per_step": cnt.rays_traced * world,
+            "reference_mrays_per_s": cnt.rays_traced * world / (ms_wf * 1e-3) / 1e6,
             "megakernel": {"value": mk_value, "unit": "Mpaths/s", "ms_per_step": ms_mk,
                            "tree": "4-wide (the tree the wavefront walks)"},
             "megakernel_binary_tree": {"value": paths_per_frame * world / (ms_mk_bin * 1e-3) / 1e6,
@@ -773,9 +777,9 @@ def measure_mesh(ctx, stream) -> dict:
     st.engine = A.ENGINE_WAVEFRONT
     wf_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 2)
     cnt = RenderStats()
-    st.count_rays = True
+    st.count_rays, st.count_nodes = True, True
     ctx.render(sm, st, stats=cnt)
-    st.count_rays = False
+    st.count_rays, st.count_nodes = False, False
     st.engine = A.ENGINE_MEGAKERNEL
     mk_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 1)
     st.binary_tree = True
@@ -783,6 +787,32 @@ def measure_mesh(ctx, stream) -> dict:
     st.binary_tree = False
     ctx.free(sm)
     rays = cnt.extension_rays + cnt.shadow_rays
+    # the same frame with the wide traversals on a linear BVH over Pencil's
+    # leaves (pgpu_set_traversal_tree), built on the device at upload; the
+    # launch parameters tuned above
+    ctx.set_traversal_tree(A.TRAVERSAL_LBVH)
+    t0 = time.perf_counter()
+    sl = ctx.upload(wm.scene, nodes)
+    upload_lbvh_ms = (time.perf_counter() - t0) * 1e3
+    ctx.set_traversal_tree(A.TRAVERSAL_UPLOADED)
+    info_l = ctx.scene_info(sl)
+    st.engine = A.ENGINE_WAVEFRONT
+    wf_l_ms = _event_ms(stream, lambda: ctx.render_device(sl, st, buf.data_ptr()), 2)
+    cnt_l = RenderStats()
+    st.count_rays, st.count_nodes = True, True
+    ctx.render(sl, st, stats=cnt_l)
+    st.count_rays, st.count_nodes = False, False
+    st.engine = A.ENGINE_MEGAKERNEL
+    mk_l_ms = _event_ms(stream, lambda: ctx.render_device(sl, st, buf.data_ptr()), 1)
+    ctx.free(sl)
+    lbvh = {"tree": "linear BVH over Pencil's leaves (same leaf boxes and slots), built on the "
+                    "device at upload",
+            "upload_ms": upload_lbvh_ms, "wide_nodes": info_l["n_wide"],
+            "wavefront_ms": wf_l_ms, "wavefront_mpaths_s": paths / wf_l_ms / 1e3,
+            "megakernel_ms": mk_l_ms, "megakernel_mpaths_s": paths / mk_l_ms / 1e3,
+            "wavefront_over_megakernel": mk_l_ms / wf_l_ms,
+            "ext_node_visits_per_ray": cnt_l.ext_node_visits / max(1, cnt_l.extension_rays),
+            "shadow_node_visits_per_ray": cnt_l.shadow_node_visits / max(1, cnt_l.shadow_rays)}
     return {"workload": "mesh_box: displaced icosphere 1,310,720 triangles in a box, quad-light "
                         "NEE, 1024x1024, 64 spp, depth 12",
             "paths": paths, "triangles": int(len(wm.scene.mesh_indices)),
@@ -793,8 +823,11 @@ def measure_mesh(ctx, stream) -> dict:
             "megakernel_ms": mk_ms, "megakernel_mpaths_s": paths / mk_ms / 1e3,
             "megakernel_binary_tree_ms": mk_bin_ms,
             "wavefront_over_megakernel": mk_ms / wf_ms,
+            "ext_node_visits_per_ray": cnt.ext_node_visits / max(1, cnt.extension_rays),
+            "shadow_node_visits_per_ray": cnt.shadow_node_visits / max(1, cnt.shadow_rays),
             "autotuned": {k: tuned[k] for k in ("queue_capacity", "refill_below", "sort_key",
-                                                 "block_size", "ms")}}
+                                                 "block_size", "ms")},
+            "lbvh_traversal": lbvh}
 
 
 class _Null:

@@ -294,6 +294,26 @@ void*   pgpu_get_stream(pgpu_ctx* ctx);
  * answering (src/distributed.hpp:527-545). */
 int32_t pgpu_set_timeout(pgpu_ctx* ctx, int32_t ms);
 
+/* The tree the wide traversals walk (both engines), for scenes uploaded
+ * after the call. Either way the leaves are the uploaded tree's: its leaf
+ * boxes, bit for bit, and its DFS leaf order, which decides among hits at
+ * equal distance as BVHNode::hit does (src/bvh.hpp:31-37), so hit
+ * distances are the same and images agree but where rounding at a box face
+ * makes the order of the walk matter. The binary tree the upload keeps
+ * (PGPU_FLAG_BINARY_TREE, the adjoint) is the uploaded one in both modes.
+ *   PGPU_TRAVERSAL_UPLOADED (0, default): the uploaded tree (Pencil's SAH
+ *       tree), collapsed to wide nodes.
+ *   PGPU_TRAVERSAL_LBVH (1): a linear BVH over the uploaded leaves, built on
+ *       the device at upload (Morton order of the box centres), then
+ *       collapsed: on meshes where Pencil's 12-bucket split binning over the
+ *       parent box groups badly, far fewer node visits per ray.
+ * No counterpart in the reference, whose renderer walks the tree it built. */
+enum pgpu_traversal_tree {
+    PGPU_TRAVERSAL_UPLOADED = 0,
+    PGPU_TRAVERSAL_LBVH     = 1
+};
+int32_t pgpu_set_traversal_tree(pgpu_ctx* ctx, int32_t mode);
+
 /* Build the primitive's stored state from its constructor arguments, with
  * the same float arithmetic as the C++ constructors (plane normal and
  * cylinder/cone axis normalised; cylinder height halved).

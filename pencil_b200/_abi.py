@@ -38,6 +38,7 @@ FLAG_PROFILE_KERNELS = 16
 FLAG_NO_PACKETS = 32
 FLAG_MIS = 64
 FLAG_BINARY_TREE = 128
+TRAVERSAL_UPLOADED, TRAVERSAL_LBVH = 0, 1
 TONEMAP_NONE, TONEMAP_ACES, TONEMAP_REINHARD = 0, 1, 2
 TONEMAP_DEVICE_INPUT, TONEMAP_DEVICE_OUTPUT = 1, 2
 KERNEL_CLASSES = ("generate", "extend", "shade", "shadow", "accumulate", "megakernel")
@@ -114,6 +115,7 @@ EXPORTS = {
     "pgpu_set_stream": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "pgpu_get_stream": (C.c_void_p, [C.c_void_p]),
     "pgpu_set_timeout": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "pgpu_set_traversal_tree": (C.c_int32, [C.c_void_p, C.c_int32]),
     "pgpu_make_prim": (C.c_int32, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_float, C.c_float, C.c_void_p]),
     "pgpu_build_bvh": (C.c_int32, [C.POINTER(SceneDesc), C.c_void_p, C.POINTER(C.c_int32),

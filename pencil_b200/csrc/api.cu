@@ -157,6 +157,10 @@ struct pgpu_ctx {
     // and whether work of a call that ran out of it may still be running
     int timeout_ms = 0;
     bool in_flight = false;
+    // tree of the wide traversals of later uploads (pgpu_set_traversal_tree)
+    int traversal = PGPU_TRAVERSAL_UPLOADED;
+    std::vector<pgpu_bvh_node> ws_trav;
+    std::vector<int> ws_leaf_of_prim;
 };
 
 namespace {
@@ -453,6 +457,14 @@ int32_t pgpu_set_timeout(pgpu_ctx* c, int32_t ms) {
     return PGPU_OK;
 }
 
+int32_t pgpu_set_traversal_tree(pgpu_ctx* c, int32_t mode) {
+    if (!c) return PGPU_ERR_INVALID_ARG;
+    if (mode != PGPU_TRAVERSAL_UPLOADED && mode != PGPU_TRAVERSAL_LBVH)
+        return fail(c, PGPU_ERR_INVALID_ARG, "unknown traversal tree %d", mode);
+    c->traversal = mode;
+    return PGPU_OK;
+}
+
 int32_t pgpu_make_prim(int32_t type, int32_t material, const float* a, const float* b,
                        const float* cc, float s0, float s1, pgpu_prim* out) {
     if (!out) return PGPU_ERR_INVALID_ARG;
@@ -480,6 +492,62 @@ int32_t pgpu_build_bvh(const pgpu_scene* s, pgpu_bvh_node* out_nodes, int32_t* o
 }
 
 }  // extern "C"
+
+// The LBVH traversal tree of an upload (PGPU_TRAVERSAL_LBVH): built on the
+// device over the scene's primitives, checked to be a DFS table over every
+// primitive once, then given the uploaded tree's leaf boxes -- the builder's
+// boxes are the same primitive boxes; where one differs in a bit, the
+// uploaded one is taken and the interior boxes are refit as unions, so
+// every box still contains its subtree's. leaf_of[p] receives the uploaded
+// tree's leaf of primitive p.
+static int traversal_lbvh(pgpu_ctx* c, const pgpu_scene& s, const pgpu_bvh_node* nodes,
+                          int n_nodes, int nU, std::vector<int>& leaf_of,
+                          std::vector<pgpu_bvh_node>& T) {
+    leaf_of.assign(nU, -1);
+    parallel_for(n_nodes, [&](int b, int e) {
+        for (int k = b; k < e; ++k)
+            if (nodes[k].left < 0) leaf_of[nodes[k].right] = k;
+    });
+    T.resize(n_nodes);
+    int depth = 0;
+    const cudaError_t e = device_lbvh(s, nU, T.data(), depth, c->stream, c->pool);
+    if (e != cudaSuccess) return cuda_fail(c, e, "traversal tree build");
+    std::vector<char>& seen = c->ws_seen;
+    seen.assign(nU, 0);
+    std::atomic<int> bad{0}, differ{0};
+    parallel_for(n_nodes, [&](int b, int e2) {
+        for (int k = b; k < e2; ++k) {
+            const pgpu_bvh_node& t = T[k];
+            if (t.left >= 0) {
+                if (t.left != k + 1 || t.right <= k + 1 || t.right >= n_nodes) bad = 1;
+                continue;
+            }
+            if (t.right < 0 || t.right >= nU || leaf_of[t.right] < 0) { bad = 1; continue; }
+            // one leaf per primitive: a primitive's flag is set by one leaf only
+            if (__atomic_exchange_n(&seen[t.right], (char)1, __ATOMIC_RELAXED)) { bad = 1; continue; }
+            const pgpu_bvh_node& u = nodes[leaf_of[t.right]];
+            if (std::memcmp(t.bmin, u.bmin, 12) || std::memcmp(t.bmax, u.bmax, 12)) differ = 1;
+        }
+    });
+    if (bad) return fail(c, PGPU_ERR_BVH_INVALID, "device traversal tree is not a DFS table");
+    if (differ) {
+        for (int k = n_nodes - 1; k >= 0; --k) {
+            pgpu_bvh_node& t = T[k];
+            if (t.left < 0) {
+                const pgpu_bvh_node& u = nodes[leaf_of[t.right]];
+                std::memcpy(t.bmin, u.bmin, 12);
+                std::memcpy(t.bmax, u.bmax, 12);
+                continue;
+            }
+            const pgpu_bvh_node &l = T[t.left], &r = T[t.right];
+            for (int a = 0; a < 3; ++a) {
+                t.bmin[a] = std::fmin(l.bmin[a], r.bmin[a]);
+                t.bmax[a] = std::fmax(l.bmax[a], r.bmax[a]);
+            }
+        }
+    }
+    return PGPU_OK;
+}
 
 // pgpu_build_bvh_device / _sah: `sah` selects Pencil's binned SAH, else the LBVH.
 static int32_t build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node* out_nodes,
@@ -785,17 +853,29 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         return cuda_fail(c, e, "scene upload");
     }
 
-    // 4-wide nodes for the wavefront's traversal, built while the main part
-    // is in flight
+    // The tree the wide traversals walk: the uploaded one, or a linear BVH
+    // over its leaves built on the device (pgpu_set_traversal_tree). Its
+    // leaves keep the uploaded tree's leaf boxes and slots.
+    const pgpu_bvh_node* tnodes = nodes;
+    std::vector<int>& leaf_of = c->ws_leaf_of_prim;    // primitive -> its leaf in `nodes`
+    const bool lbvh = c->traversal == PGPU_TRAVERSAL_LBVH && nU >= 2;
+    if (lbvh) {
+        rc = traversal_lbvh(c, *s, nodes, n_nodes, nU, leaf_of, c->ws_trav);
+        if (rc) { release(); return rc; }
+        tnodes = c->ws_trav.data();
+    }
+    // 4-wide nodes, built while the main part is in flight
     std::vector<int>& leaf_ref = c->ws_leaf_ref;
     leaf_ref.resize(n_nodes);
     parallel_for(n_nodes, [&](int b, int e2) {
-        for (int k = b; k < e2; ++k) leaf_ref[k] = nodes[k].left < 0 ? ref_of(k) : 0;
+        for (int k = b; k < e2; ++k)
+            leaf_ref[k] = tnodes[k].left >= 0 ? 0
+                          : ref_of(lbvh ? leaf_of[tnodes[k].right] : k);
     });
     int wide_stack = 0;
     float4* h_wide = reinterpret_cast<float4*>(host + total);
-    const int n_wide = collapse_wide(nodes, n_nodes, leaf_ref, kMaxDepth, h_wide, c->ws_collapse,
-                                     wide_stack);
+    const int n_wide = collapse_wide(tnodes, n_nodes, leaf_ref, kMaxDepth, h_wide,
+                                     c->ws_collapse, wide_stack);
     if (wide_stack > kMaxDepth) {
         release();
         return fail(c, PGPU_ERR_UNSUPPORTED, "BVH needs %d stack entries, more than %d",

@@ -507,6 +507,14 @@ struct TravStack {
         if (sp < kShared) { ref = sref[sp * stride]; t = st[sp * stride]; }
         else { ref = lref[sp - kShared]; t = lt[sp - kShared]; }
     }
+    // any hit: the entries carry no distance
+    __device__ __forceinline__ void push_ref(int sp, int ref) {
+        if (sp < kShared) sref[sp * stride] = ref;
+        else lref[sp - kShared] = ref;
+    }
+    __device__ __forceinline__ int pop_ref(int sp) const {
+        return sp < kShared ? sref[sp * stride] : lref[sp - kShared];
+    }
 };
 
 // Resumable closest-hit traversal: init() tests the root, step() processes
@@ -644,8 +652,8 @@ struct AnyTrav {
             hR = false;
         }
         if (hL && hR) {
-            if (eR < eL) { stk.push(sp, rr.x, 0.0f); node = rr.y; }
-            else { stk.push(sp, rr.y, 0.0f); node = rr.x; }
+            if (eR < eL) { stk.push_ref(sp, rr.x); node = rr.y; }
+            else { stk.push_ref(sp, rr.y); node = rr.x; }
             ++sp;
             return false;
         }
@@ -653,8 +661,7 @@ struct AnyTrav {
         if (hR) { node = rr.y; return false; }
         if (sp == 0) return true;
         --sp;
-        float te;
-        stk.pop(sp, node, te);
+        node = stk.pop_ref(sp);
         return false;
     }
 };
@@ -814,9 +821,15 @@ __device__ __forceinline__ int push_children(const WideNode& w, unsigned im,
         float k3 = (im & 8u) ? e[3] : INFINITY;
         int r0 = w.ref[0].x, r1 = w.ref[0].y, r2 = w.ref[0].z, r3 = w.ref[0].w;
         sort4(k0, r0, k1, r1, k2, r2, k3, r3);
-        if (k3 != INFINITY) stk.push(sp++, r3, keyed ? k3 : 0.0f);
-        if (k2 != INFINITY) stk.push(sp++, r2, keyed ? k2 : 0.0f);
-        if (k1 != INFINITY) stk.push(sp++, r1, keyed ? k1 : 0.0f);
+        if (keyed) {
+            if (k3 != INFINITY) stk.push(sp++, r3, k3);
+            if (k2 != INFINITY) stk.push(sp++, r2, k2);
+            if (k1 != INFINITY) stk.push(sp++, r1, k1);
+        } else {
+            if (k3 != INFINITY) stk.push_ref(sp++, r3);
+            if (k2 != INFINITY) stk.push_ref(sp++, r2);
+            if (k1 != INFINITY) stk.push_ref(sp++, r1);
+        }
         return r0;
     } else if (!keyed) {
         // any hit: the nearest child next, the others in child order
@@ -829,7 +842,7 @@ __device__ __forceinline__ int push_children(const WideNode& w, unsigned im,
         while (im) {
             const int k = 31 - __clz(im);
             im &= ~(1u << k);
-            stk.push(sp++, pick_ref(w, k), 0.0f);
+            stk.push_ref(sp++, pick_ref(w, k));
         }
         return pick_ref(w, kn);
     } else {
@@ -981,8 +994,7 @@ struct AnyTrav4 {
         }
         if (sp == 0) return true;
         --sp;
-        float te;
-        stk.pop(sp, node, te);
+        node = stk.pop_ref(sp);
         return false;
     }
 };
@@ -1082,8 +1094,8 @@ __device__ bool any_hit(const SceneView& S, const Ray& ray, float tmin, float tm
         if (hL && rr.x < 0) { if (test_leaf(rr.x)) return true; hL = false; }
         if (hR && rr.y < 0) { if (test_leaf(rr.y)) return true; hR = false; }
         if (hL && hR) {
-            if (eR < eL) { stk.push(sp, rr.x, 0.0f); node = rr.y; }
-            else { stk.push(sp, rr.y, 0.0f); node = rr.x; }
+            if (eR < eL) { stk.push_ref(sp, rr.x); node = rr.y; }
+            else { stk.push_ref(sp, rr.y); node = rr.x; }
             ++sp;
         } else if (hL) {
             node = rr.x;
@@ -1092,8 +1104,7 @@ __device__ bool any_hit(const SceneView& S, const Ray& ray, float tmin, float tm
         } else {
             if (sp == 0) return false;
             --sp;
-            float te;
-            stk.pop(sp, node, te);
+            node = stk.pop_ref(sp);
         }
     }
 }

@@ -141,6 +141,13 @@ class GpuContext:
         """Wall-clock budget of a render's device work (0: none)."""
         self.check(self.lib.pgpu_set_timeout(self.h, int(ms)), "pgpu_set_timeout")
 
+    def set_traversal_tree(self, mode: int) -> None:
+        """Tree the wide traversals of later uploads walk:
+        A.TRAVERSAL_UPLOADED (the uploaded tree, default) or A.TRAVERSAL_LBVH
+        (a linear BVH over the uploaded leaves, built on the device)."""
+        self.check(self.lib.pgpu_set_traversal_tree(self.h, int(mode)),
+                   "pgpu_set_traversal_tree")
+
     def upload(self, scene: Scene, nodes: np.ndarray | None = None,
                camera: CameraArgs | None = None) -> int:
         d, keep = scene.desc(nodes, camera)
