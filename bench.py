@@ -67,6 +67,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint, batch and image-quality measurements")
+    ap.add_argument("--profile-pencil-tree", action="store_true",
+                    help="mesh profile case: the wide traversals on Pencil's tree")
     ap.add_argument("--profile-case", choices=["wavefront", "megakernel", "mesh", "adjoint",
                                                "lbvh", "tonemap"], default=None,
                     help="render the workload once, kernels launched one by one (for ncu)")
@@ -680,7 +682,11 @@ def measure_quality(ctx, sid, st, stream) -> dict:
     # mesh box at 256x256
     wm = W.mesh_box(width=256, height=256)
     nodes, _ = wm.scene.build_bvh()
-    sm = ctx.upload(wm.scene, nodes)
+    ctx.set_traversal_tree(A.TRAVERSAL_LBVH)      # the mesh's configuration (measure_mesh)
+    try:
+        sm = ctx.upload(wm.scene, nodes)
+    finally:
+        ctx.set_traversal_tree(A.TRAVERSAL_UPLOADED)
     sm_st = dataclasses.replace(wm.settings, engine=A.ENGINE_WAVEFRONT)
     mwin = (0, 0, 256, 256)
     t0 = time.perf_counter()
@@ -754,80 +760,82 @@ def measure_mesh(ctx, stream) -> dict:
     """The triangle-mesh configuration: a displaced icosphere (8
     subdivisions, 1,310,720 triangles, float32 vertices, int32 indices) in a
     box lit by a 0.25 x 0.25 emissive ceiling quad with next-event
-    estimation; 1024x1024, 64 spp, depth 12 (67,108,864 paths per frame)."""
+    estimation; 1024x1024, 64 spp, depth 12 (67,108,864 paths per frame).
+
+    Uploaded with Pencil's SAH tree (built at parse time), the wide
+    traversals walking a linear BVH over its leaves (PGPU_TRAVERSAL_LBVH,
+    built on the device at upload): the renderer's configuration for this
+    workload, autotuned, both engines on that tree. The same frame on
+    Pencil's own tree (collapsed) is measured beside it with the same
+    launch parameters, and the megakernel on Pencil's binary tree."""
     import time
 
     import torch
     from pencil_b200 import _abi as A
     from pencil_b200 import workloads as W
+    from pencil_b200.autotune import autotune
     from pencil_b200.renderer import RenderStats
     wm = W.mesh_box()
     nodes, depth = wm.scene.build_bvh()       # Pencil builds its tree at parse time
-    t0 = time.perf_counter()
-    sm = ctx.upload(wm.scene, nodes)
-    upload_ms = (time.perf_counter() - t0) * 1e3
-    info = ctx.scene_info(sm)
     st = wm.settings
     paths = st.width * st.height * st.samples ** 2
-    # launch parameters for this workload from the autotuner (capacity
-    # candidates up to 2^26 paths: the whole frame in one chunk)
-    from pencil_b200.autotune import autotune
-    tuned = autotune(ctx, [sm], [st], scene=wm.scene, reps=1, use_cache=False)
     buf = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")
-    st.engine = A.ENGINE_WAVEFRONT
-    wf_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 2)
-    cnt = RenderStats()
-    st.count_rays, st.count_nodes = True, True
-    ctx.render(sm, st, stats=cnt)
-    st.count_rays, st.count_nodes = False, False
-    st.engine = A.ENGINE_MEGAKERNEL
-    mk_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 1)
-    st.binary_tree = True
-    mk_bin_ms = _event_ms(stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 1)
-    st.binary_tree = False
-    ctx.free(sm)
-    rays = cnt.extension_rays + cnt.shadow_rays
-    # the same frame with the wide traversals on a linear BVH over Pencil's
-    # leaves (pgpu_set_traversal_tree), built on the device at upload; the
-    # launch parameters tuned above
+
+    def frame(sid) -> dict:
+        st.engine = A.ENGINE_WAVEFRONT
+        wf = _event_ms(stream, lambda: ctx.render_device(sid, st, buf.data_ptr()), 2)
+        cnt = RenderStats()
+        st.count_rays, st.count_nodes = True, True
+        ctx.render(sid, st, stats=cnt)
+        st.count_rays, st.count_nodes = False, False
+        st.engine = A.ENGINE_MEGAKERNEL
+        mk = _event_ms(stream, lambda: ctx.render_device(sid, st, buf.data_ptr()), 1)
+        st.engine = A.ENGINE_WAVEFRONT
+        rays = cnt.extension_rays + cnt.shadow_rays
+        return {"wavefront_ms": wf, "wavefront_mpaths_s": paths / wf / 1e3,
+                "wavefront_mrays_s": rays / wf / 1e3,
+                "megakernel_ms": mk, "megakernel_mpaths_s": paths / mk / 1e3,
+                "wavefront_over_megakernel": mk / wf,
+                "ext_node_visits_per_ray": cnt.ext_node_visits / max(1, cnt.extension_rays),
+                "shadow_node_visits_per_ray": cnt.shadow_node_visits / max(1, cnt.shadow_rays)}
+
+    # the renderer's configuration: LBVH traversal tree over Pencil's leaves
     ctx.set_traversal_tree(A.TRAVERSAL_LBVH)
-    t0 = time.perf_counter()
-    sl = ctx.upload(wm.scene, nodes)
-    upload_lbvh_ms = (time.perf_counter() - t0) * 1e3
-    ctx.set_traversal_tree(A.TRAVERSAL_UPLOADED)
-    info_l = ctx.scene_info(sl)
-    st.engine = A.ENGINE_WAVEFRONT
-    wf_l_ms = _event_ms(stream, lambda: ctx.render_device(sl, st, buf.data_ptr()), 2)
-    cnt_l = RenderStats()
-    st.count_rays, st.count_nodes = True, True
-    ctx.render(sl, st, stats=cnt_l)
-    st.count_rays, st.count_nodes = False, False
-    st.engine = A.ENGINE_MEGAKERNEL
-    mk_l_ms = _event_ms(stream, lambda: ctx.render_device(sl, st, buf.data_ptr()), 1)
+    try:
+        t0 = time.perf_counter()
+        sl = ctx.upload(wm.scene, nodes)
+        upload_ms = (time.perf_counter() - t0) * 1e3
+    finally:
+        ctx.set_traversal_tree(A.TRAVERSAL_UPLOADED)
+    info = ctx.scene_info(sl)
+    # launch parameters from the autotuner (capacity candidates up to 2^26
+    # paths: the whole frame in one chunk)
+    tuned = autotune(ctx, [sl], [st], scene=wm.scene, reps=1, use_cache=False)
+    head = frame(sl)
     ctx.free(sl)
-    lbvh = {"tree": "linear BVH over Pencil's leaves (same leaf boxes and slots), built on the "
-                    "device at upload",
-            "upload_ms": upload_lbvh_ms, "wide_nodes": info_l["n_wide"],
-            "wavefront_ms": wf_l_ms, "wavefront_mpaths_s": paths / wf_l_ms / 1e3,
-            "megakernel_ms": mk_l_ms, "megakernel_mpaths_s": paths / mk_l_ms / 1e3,
-            "wavefront_over_megakernel": mk_l_ms / wf_l_ms,
-            "ext_node_visits_per_ray": cnt_l.ext_node_visits / max(1, cnt_l.extension_rays),
-            "shadow_node_visits_per_ray": cnt_l.shadow_node_visits / max(1, cnt_l.shadow_rays)}
+    # Pencil's own tree, collapsed, with the same launch parameters
+    t0 = time.perf_counter()
+    sm = ctx.upload(wm.scene, nodes)
+    upload_pencil_ms = (time.perf_counter() - t0) * 1e3
+    pencil = {"tree": "Pencil's SAH tree, collapsed to 4-wide nodes",
+              "upload_ms": upload_pencil_ms, "wide_nodes": ctx.scene_info(sm)["n_wide"],
+              **frame(sm)}
+    st.engine, st.binary_tree = A.ENGINE_MEGAKERNEL, True
+    pencil["megakernel_binary_tree_ms"] = _event_ms(
+        stream, lambda: ctx.render_device(sm, st, buf.data_ptr()), 1)
+    st.engine, st.binary_tree = A.ENGINE_WAVEFRONT, False
+    ctx.free(sm)
     return {"workload": "mesh_box: displaced icosphere 1,310,720 triangles in a box, quad-light "
                         "NEE, 1024x1024, 64 spp, depth 12",
             "paths": paths, "triangles": int(len(wm.scene.mesh_indices)),
-            "bvh_depth": int(depth), "wide_nodes": info["n_wide"],
-            "device_bytes": info["device_bytes"], "upload_ms": upload_ms,
-            "wavefront_ms": wf_ms, "wavefront_mpaths_s": paths / wf_ms / 1e3,
-            "wavefront_mrays_s": rays / wf_ms / 1e3,
-            "megakernel_ms": mk_ms, "megakernel_mpaths_s": paths / mk_ms / 1e3,
-            "megakernel_binary_tree_ms": mk_bin_ms,
-            "wavefront_over_megakernel": mk_ms / wf_ms,
-            "ext_node_visits_per_ray": cnt.ext_node_visits / max(1, cnt.extension_rays),
-            "shadow_node_visits_per_ray": cnt.shadow_node_visits / max(1, cnt.shadow_rays),
+            "bvh_depth": int(depth),
+            "traversal_tree": "linear BVH over Pencil's leaves (their boxes and DFS order: the "
+                              "same hits), built on the device at upload",
+            "wide_nodes": info["n_wide"], "device_bytes": info["device_bytes"],
+            "upload_ms": upload_ms, **head,
             "autotuned": {k: tuned[k] for k in ("queue_capacity", "refill_below", "sort_key",
                                                  "block_size", "ms")},
-            "lbvh_traversal": lbvh}
+            "pencil_tree": pencil}
 
 
 class _Null:
@@ -873,17 +881,18 @@ def run_profile_case(args) -> None:
     st.width //= args.profile_scale
     st.height //= args.profile_scale
     st.use_graph = False
-    # the launch parameters the autotuner picks for the workload: sphere
-    # cloud one chunk, refill at 16 busy lanes; mesh chunks of 2^24 paths,
-    # refill at 20; shadow work and extension rays sorted by origin cell
-    # (sort key 3)
-    if mesh:
-        st.queue_capacity, st.refill_below = 1 << 24, 20
-    else:
-        st.queue_capacity, st.refill_below = st.width * st.height * st.samples ** 2, 16
+    # the launch parameters the autotuner picks for the workload: one chunk
+    # (the whole frame), refill at 16 busy lanes (sphere cloud) or 20 (mesh),
+    # shadow work and extension rays sorted by origin cell (sort key 3); the
+    # mesh's wide traversals on the LBVH over Pencil's leaves (its bench
+    # configuration) unless --profile-pencil-tree
+    st.queue_capacity = st.width * st.height * st.samples ** 2
+    st.refill_below = 20 if mesh else 16
     st.sort_key = 3
     st.engine = A.ENGINE_MEGAKERNEL if args.profile_case == "megakernel" else A.ENGINE_WAVEFRONT
     ctx = GpuContext(0)
+    if mesh and not args.profile_pencil_tree:
+        ctx.set_traversal_tree(A.TRAVERSAL_LBVH)
     sid = ctx.upload(wl.scene, wl.scene.build_bvh()[0] if mesh else None)
     stats = RenderStats()
     img = ctx.render(sid, st, stats=stats)
