@@ -307,10 +307,15 @@ int32_t pgpu_set_timeout(pgpu_ctx* ctx, int32_t ms);
  *       the device at upload (Morton order of the box centres), then
  *       collapsed: on meshes where Pencil's 12-bucket split binning over the
  *       parent box groups badly, far fewer node visits per ray.
+ *   PGPU_TRAVERSAL_SAH (2): a binned SAH tree over the uploaded leaves,
+ *       built on the device at upload: 16 buckets over each node's centroid
+ *       bounds on all three axes, Pencil's cost function, one primitive per
+ *       leaf; slower to build than the LBVH, fewer node visits.
  * No counterpart in the reference, whose renderer walks the tree it built. */
 enum pgpu_traversal_tree {
     PGPU_TRAVERSAL_UPLOADED = 0,
-    PGPU_TRAVERSAL_LBVH     = 1
+    PGPU_TRAVERSAL_LBVH     = 1,
+    PGPU_TRAVERSAL_SAH      = 2
 };
 int32_t pgpu_set_traversal_tree(pgpu_ctx* ctx, int32_t mode);
 

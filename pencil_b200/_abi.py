@@ -38,7 +38,7 @@ FLAG_PROFILE_KERNELS = 16
 FLAG_NO_PACKETS = 32
 FLAG_MIS = 64
 FLAG_BINARY_TREE = 128
-TRAVERSAL_UPLOADED, TRAVERSAL_LBVH = 0, 1
+TRAVERSAL_UPLOADED, TRAVERSAL_LBVH, TRAVERSAL_SAH = 0, 1, 2
 TONEMAP_NONE, TONEMAP_ACES, TONEMAP_REINHARD = 0, 1, 2
 TONEMAP_DEVICE_INPUT, TONEMAP_DEVICE_OUTPUT = 1, 2
 KERNEL_CLASSES = ("generate", "extend", "shade", "shadow", "accumulate", "megakernel")

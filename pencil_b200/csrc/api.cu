@@ -49,7 +49,7 @@ cudaError_t launch_tonemap(const float* d_hdr, long long n_pixels, int mode, flo
                            uint8_t* d_out, const float* d_thr, cudaStream_t st);
 const float* gamma_thresholds_host();
 cudaError_t device_sah(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, int& depth,
-                       cudaStream_t st, cudaMemPool_t pool);
+                       cudaStream_t st, cudaMemPool_t pool, bool quality);
 cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, int& depth,
                         cudaStream_t st, cudaMemPool_t pool);
 
@@ -459,7 +459,8 @@ int32_t pgpu_set_timeout(pgpu_ctx* c, int32_t ms) {
 
 int32_t pgpu_set_traversal_tree(pgpu_ctx* c, int32_t mode) {
     if (!c) return PGPU_ERR_INVALID_ARG;
-    if (mode != PGPU_TRAVERSAL_UPLOADED && mode != PGPU_TRAVERSAL_LBVH)
+    if (mode != PGPU_TRAVERSAL_UPLOADED && mode != PGPU_TRAVERSAL_LBVH &&
+        mode != PGPU_TRAVERSAL_SAH)
         return fail(c, PGPU_ERR_INVALID_ARG, "unknown traversal tree %d", mode);
     c->traversal = mode;
     return PGPU_OK;
@@ -493,15 +494,15 @@ int32_t pgpu_build_bvh(const pgpu_scene* s, pgpu_bvh_node* out_nodes, int32_t* o
 
 }  // extern "C"
 
-// The LBVH traversal tree of an upload (PGPU_TRAVERSAL_LBVH): built on the
+// The traversal tree of an upload (PGPU_TRAVERSAL_LBVH / _SAH): built on the
 // device over the scene's primitives, checked to be a DFS table over every
 // primitive once, then given the uploaded tree's leaf boxes -- the builder's
 // boxes are the same primitive boxes; where one differs in a bit, the
 // uploaded one is taken and the interior boxes are refit as unions, so
 // every box still contains its subtree's. leaf_of[p] receives the uploaded
 // tree's leaf of primitive p.
-static int traversal_lbvh(pgpu_ctx* c, const pgpu_scene& s, const pgpu_bvh_node* nodes,
-                          int n_nodes, int nU, std::vector<int>& leaf_of,
+static int traversal_tree(pgpu_ctx* c, const pgpu_scene& s, const pgpu_bvh_node* nodes,
+                          int n_nodes, int nU, int mode, std::vector<int>& leaf_of,
                           std::vector<pgpu_bvh_node>& T) {
     leaf_of.assign(nU, -1);
     parallel_for(n_nodes, [&](int b, int e) {
@@ -510,7 +511,9 @@ static int traversal_lbvh(pgpu_ctx* c, const pgpu_scene& s, const pgpu_bvh_node*
     });
     T.resize(n_nodes);
     int depth = 0;
-    const cudaError_t e = device_lbvh(s, nU, T.data(), depth, c->stream, c->pool);
+    const cudaError_t e = mode == PGPU_TRAVERSAL_SAH
+                              ? device_sah(s, nU, T.data(), depth, c->stream, c->pool, true)
+                              : device_lbvh(s, nU, T.data(), depth, c->stream, c->pool);
     if (e != cudaSuccess) return cuda_fail(c, e, "traversal tree build");
     std::vector<char>& seen = c->ws_seen;
     seen.assign(nU, 0);
@@ -582,7 +585,7 @@ static int32_t build_bvh_device(pgpu_ctx* c, const pgpu_scene* s, pgpu_bvh_node*
     PGPU_CUDA(c, cudaSetDevice(c->device));
     PGPU_CUDA(c, ensure_pool(c));
     int depth = 0;
-    cudaError_t e = sah ? device_sah(*s, n, out_nodes, depth, c->stream, c->pool)
+    cudaError_t e = sah ? device_sah(*s, n, out_nodes, depth, c->stream, c->pool, false)
                         : device_lbvh(*s, n, out_nodes, depth, c->stream, c->pool);
     if (e != cudaSuccess) return cuda_fail(c, e, "device BVH build");
     if (out_depth) *out_depth = depth;
@@ -853,14 +856,14 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         return cuda_fail(c, e, "scene upload");
     }
 
-    // The tree the wide traversals walk: the uploaded one, or a linear BVH
-    // over its leaves built on the device (pgpu_set_traversal_tree). Its
-    // leaves keep the uploaded tree's leaf boxes and slots.
+    // The tree the wide traversals walk: the uploaded one, or one built on
+    // the device over its leaves (pgpu_set_traversal_tree). Its leaves keep
+    // the uploaded tree's leaf boxes and slots.
     const pgpu_bvh_node* tnodes = nodes;
     std::vector<int>& leaf_of = c->ws_leaf_of_prim;    // primitive -> its leaf in `nodes`
-    const bool lbvh = c->traversal == PGPU_TRAVERSAL_LBVH && nU >= 2;
-    if (lbvh) {
-        rc = traversal_lbvh(c, *s, nodes, n_nodes, nU, leaf_of, c->ws_trav);
+    const bool own_tree = c->traversal != PGPU_TRAVERSAL_UPLOADED && nU >= 2;
+    if (own_tree) {
+        rc = traversal_tree(c, *s, nodes, n_nodes, nU, c->traversal, leaf_of, c->ws_trav);
         if (rc) { release(); return rc; }
         tnodes = c->ws_trav.data();
     }
@@ -870,7 +873,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     parallel_for(n_nodes, [&](int b, int e2) {
         for (int k = b; k < e2; ++k)
             leaf_ref[k] = tnodes[k].left >= 0 ? 0
-                          : ref_of(lbvh ? leaf_of[tnodes[k].right] : k);
+                          : ref_of(own_tree ? leaf_of[tnodes[k].right] : k);
     });
     int wide_stack = 0;
     float4* h_wide = reinterpret_cast<float4*>(host + total);

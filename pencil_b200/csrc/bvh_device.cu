@@ -306,6 +306,10 @@ struct DevBuf {
 constexpr int kSahBuckets = 12;
 constexpr int kSahChunk = 1024;    // primitives per block of the bin / partition passes
 constexpr int kSahBlock = 256;
+// The quality variant (traversal trees, not Pencil's tree): buckets over the
+// node's centroid bounds rather than its box, on all three axes.
+constexpr int kQualBuckets = 16;
+template <bool Q> constexpr int kBinsPerTask = Q ? 3 * kQualBuckets : kSahBuckets;
 
 struct SahTask {                   // a node with more than 4 primitives
     int start, count;              // its range of the permutation
@@ -342,6 +346,23 @@ __device__ __forceinline__ int sah_bucket(const DBox& b, int axis, float lo, flo
     if (k >= kSahBuckets) k = kSahBuckets - 1;
     return k;
 }
+// Quality variant: bucket of a box centre over the node's centroid bounds
+// cb (ord() images: min x y z, max x y z) along `axis`.
+__device__ __forceinline__ int qual_bucket(const DBox& b, int axis, const int* cb) {
+    const float lo = unord(cb[axis]), hi = unord(cb[3 + axis]);
+    const float center = (b.mn[axis] + b.mx[axis]) * 0.5f;
+    int k = (int)((center - lo) / (hi - lo) * kQualBuckets);
+    if (k < 0) k = 0;
+    if (k >= kQualBuckets) k = kQualBuckets - 1;
+    return k;
+}
+// The bucket a primitive of task t falls in along the chosen axis.
+template <bool Q>
+__device__ __forceinline__ int task_bucket(const DBox& b, int axis, const SahTask& tk,
+                                           const int* cb_task) {
+    if constexpr (Q) return qual_bucket(b, axis, cb_task);
+    else return sah_bucket(b, axis, tk.mn[axis], tk.mx[axis]);
+}
 __device__ __forceinline__ float sah_key2(const DBox& b, int axis) {
     return b.mn[axis] + b.mx[axis];
 }
@@ -371,23 +392,68 @@ __global__ void sah_bins_init(SahBin* bins, int n) {
     }
 }
 
-// One block per item: the chunk's primitives into the task's 12 bins.
+// Quality variant: the centroid bounds of every task (ord() images), one
+// block per item, one atomic per bound and block.
+__global__ void sah_cb_init(int* cb, int n) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        cb[k] = (k % 6) < 3 ? ord(1e30f) : ord(-1e30f);
+}
+__global__ void __launch_bounds__(kSahBlock)
+sah_cbounds(const SahTask* tasks, int T, const int* item_off, const int* nchunk, const int* perm,
+            const DBox* boxes, int* cb) {
+    const int items = item_off[T - 1] + nchunk[T - 1];
+    if ((int)blockIdx.x >= items) return;
+    const int t = item_task(item_off, T, blockIdx.x);
+    const SahTask tk = tasks[t];
+    const int begin = tk.start + (blockIdx.x - item_off[t]) * kSahChunk;
+    const int end = min(begin + kSahChunk, tk.start + tk.count);
+    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for (int p = begin + threadIdx.x; p < end; p += blockDim.x) {
+        const DBox b = boxes[perm[p]];
+        for (int a = 0; a < 3; ++a) {
+            const int c = ord((b.mn[a] + b.mx[a]) * 0.5f);
+            mn[a] = min(mn[a], c);
+            mx[a] = max(mx[a], c);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        for (int off = 16; off > 0; off >>= 1) {
+            mn[a] = min(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
+            mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(cb + 6 * t + a, mn[a]);
+            atomicMax(cb + 6 * t + 3 + a, mx[a]);
+        }
+    }
+}
+
+// One block per item: the chunk's primitives into the task's bins -- 12
+// along the longest axis of its box (Pencil), or 16 per axis over its
+// centroid bounds on each axis where they have an extent (quality).
+template <bool Q>
 __global__ void __launch_bounds__(kSahBlock)
 sah_bin(const SahTask* tasks, int T, const int* item_off, const int* nchunk, const int* perm,
-        const DBox* boxes, SahBin* bins) {
-    __shared__ int s_cnt[kSahBuckets], s_mn[kSahBuckets][3], s_mx[kSahBuckets][3];
+        const DBox* boxes, const int* cb, SahBin* bins) {
+    constexpr int NB = kBinsPerTask<Q>;
+    __shared__ int s_cnt[NB], s_mn[NB][3], s_mx[NB][3];
     const int items = item_off[T - 1] + nchunk[T - 1];
     if ((int)blockIdx.x >= items) return;
     const int t = item_task(item_off, T, blockIdx.x);
     const SahTask tk = tasks[t];
     const int axis = sah_axis(tk.mn, tk.mx);
-    const float lo = tk.mn[axis], hi = tk.mx[axis];
-    if (!(hi > lo)) return;                      // median split: no bins
-    if (threadIdx.x < kSahBuckets) {
-        s_cnt[threadIdx.x] = 0;
+    bool on_axis[3] = {false, false, false};
+    if constexpr (Q) {
+        for (int a = 0; a < 3; ++a) on_axis[a] = unord(cb[6 * t + 3 + a]) > unord(cb[6 * t + a]);
+        if (!on_axis[0] && !on_axis[1] && !on_axis[2]) return;   // median split: no bins
+    } else {
+        if (!(tk.mx[axis] > tk.mn[axis])) return;                 // median split: no bins
+    }
+    for (int k = threadIdx.x; k < NB; k += blockDim.x) {
+        s_cnt[k] = 0;
         for (int a = 0; a < 3; ++a) {
-            s_mn[threadIdx.x][a] = ord(1e30f);
-            s_mx[threadIdx.x][a] = ord(-1e30f);
+            s_mn[k][a] = ord(1e30f);
+            s_mx[k][a] = ord(-1e30f);
         }
     }
     __syncthreads();
@@ -395,28 +461,90 @@ sah_bin(const SahTask* tasks, int T, const int* item_off, const int* nchunk, con
     const int end = min(begin + kSahChunk, tk.start + tk.count);
     for (int p = begin + threadIdx.x; p < end; p += blockDim.x) {
         const DBox b = boxes[perm[p]];
-        const int k = sah_bucket(b, axis, lo, hi);
-        atomicAdd(&s_cnt[k], 1);
-        for (int a = 0; a < 3; ++a) {
-            atomicMin(&s_mn[k][a], ord(b.mn[a]));
-            atomicMax(&s_mx[k][a], ord(b.mx[a]));
+        auto put = [&](int k) {
+            atomicAdd(&s_cnt[k], 1);
+            for (int a = 0; a < 3; ++a) {
+                atomicMin(&s_mn[k][a], ord(b.mn[a]));
+                atomicMax(&s_mx[k][a], ord(b.mx[a]));
+            }
+        };
+        if constexpr (Q) {
+            for (int ax = 0; ax < 3; ++ax)
+                if (on_axis[ax]) put(ax * kQualBuckets + qual_bucket(b, ax, cb + 6 * t));
+        } else {
+            put(sah_bucket(b, axis, tk.mn[axis], tk.mx[axis]));
         }
     }
     __syncthreads();
-    if (threadIdx.x < kSahBuckets && s_cnt[threadIdx.x] > 0) {
-        SahBin* g = bins + (size_t)t * kSahBuckets + threadIdx.x;
-        atomicAdd(&g->count, s_cnt[threadIdx.x]);
+    for (int k = threadIdx.x; k < NB; k += blockDim.x) {
+        if (s_cnt[k] == 0) continue;
+        SahBin* g = bins + (size_t)t * NB + k;
+        atomicAdd(&g->count, s_cnt[k]);
         for (int a = 0; a < 3; ++a) {
-            atomicMin(&g->mn[a], s_mn[threadIdx.x][a]);
-            atomicMax(&g->mx[a], s_mx[threadIdx.x][a]);
+            atomicMin(&g->mn[a], s_mn[k][a]);
+            atomicMax(&g->mx[a], s_mx[k][a]);
         }
     }
 }
 
-// One thread per task: sah_split's choice (src/bvh.hpp:119-192), or the
-// median split when the axis has no extent or no boundary separates.
-__global__ void sah_choose(const SahTask* tasks, int T, const SahBin* bins, SahChoice* ch,
-                           int* fb_list, int* n_fb) {
+// The cheapest boundary among `nb` bins (prefix / suffix merges, cost
+// 1 + (nL SA_L + nR SA_R) / SA_P with the reference's operations in its
+// order); updates c and best_cost when a boundary beats best_cost.
+__device__ __forceinline__ void sah_best_boundary(const SahBin* b, int nb, int axis,
+                                                  float sa_parent, SahChoice& c,
+                                                  float& best_cost) {
+    float pmn[kQualBuckets + 1][3], pmx[kQualBuckets + 1][3];
+    float smn[kQualBuckets + 1][3], smx[kQualBuckets + 1][3];
+    int pc[kQualBuckets + 1], sc[kQualBuckets + 1];
+    for (int a = 0; a < 3; ++a) {
+        pmn[0][a] = smn[nb][a] = 1e30f;
+        pmx[0][a] = smx[nb][a] = -1e30f;
+    }
+    pc[0] = sc[nb] = 0;
+    for (int i = 0; i < nb; ++i) {
+        for (int a = 0; a < 3; ++a) {
+            pmn[i + 1][a] = fminf(pmn[i][a], unord(b[i].mn[a]));
+            pmx[i + 1][a] = fmaxf(pmx[i][a], unord(b[i].mx[a]));
+        }
+        pc[i + 1] = pc[i] + b[i].count;
+    }
+    for (int i = nb - 1; i >= 0; --i) {
+        for (int a = 0; a < 3; ++a) {
+            smn[i][a] = fminf(smn[i + 1][a], unord(b[i].mn[a]));
+            smx[i][a] = fmaxf(smx[i + 1][a], unord(b[i].mx[a]));
+        }
+        sc[i] = sc[i + 1] + b[i].count;
+    }
+    for (int i = 1; i < nb; ++i) {
+        const int nL = pc[i], nR = sc[i];
+        if (nL == 0 || nR == 0) continue;
+        const float sa_l = sah_area(pmn[i], pmx[i]);
+        const float sa_r = sah_area(smn[i], smx[i]);
+        const float cost =
+            1.0f + ((float)nL * sa_l + (float)nR * sa_r) / (sa_parent > 0 ? sa_parent : 1.0f);
+        if (cost < best_cost) {
+            best_cost = cost;
+            c.mode = 0;
+            c.axis = axis;
+            c.best = i;
+            c.nl = nL;
+            for (int a = 0; a < 3; ++a) {
+                c.lmn[a] = pmn[i][a];
+                c.lmx[a] = pmx[i][a];
+                c.rmn[a] = smn[i][a];
+                c.rmx[a] = smx[i][a];
+            }
+        }
+    }
+}
+
+// One thread per task: sah_split's choice (src/bvh.hpp:119-192) -- or, in
+// the quality variant, the best boundary over the three axes' bins -- or the
+// median split along the box's longest axis when no boundary separates.
+template <bool Q>
+__global__ void sah_choose(const SahTask* tasks, int T, const SahBin* bins, const int* cb,
+                           SahChoice* ch, int* fb_list, int* n_fb) {
+    constexpr int NB = kBinsPerTask<Q>;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         const SahTask tk = tasks[t];
         SahChoice c;
@@ -424,55 +552,18 @@ __global__ void sah_choose(const SahTask* tasks, int T, const SahBin* bins, SahC
         c.mode = 1;
         c.best = -1;
         c.nl = tk.count / 2;
-        const float lo = tk.mn[c.axis], hi = tk.mx[c.axis];
-        if (hi > lo) {
-            float pmn[kSahBuckets + 1][3], pmx[kSahBuckets + 1][3];
-            float smn[kSahBuckets + 1][3], smx[kSahBuckets + 1][3];
-            int pc[kSahBuckets + 1], sc[kSahBuckets + 1];
-            for (int a = 0; a < 3; ++a) {
-                pmn[0][a] = smn[kSahBuckets][a] = 1e30f;
-                pmx[0][a] = smx[kSahBuckets][a] = -1e30f;
-            }
-            pc[0] = sc[kSahBuckets] = 0;
-            const SahBin* b = bins + (size_t)t * kSahBuckets;
-            for (int i = 0; i < kSahBuckets; ++i) {
-                for (int a = 0; a < 3; ++a) {
-                    pmn[i + 1][a] = fminf(pmn[i][a], unord(b[i].mn[a]));
-                    pmx[i + 1][a] = fmaxf(pmx[i][a], unord(b[i].mx[a]));
-                }
-                pc[i + 1] = pc[i] + b[i].count;
-            }
-            for (int i = kSahBuckets - 1; i >= 0; --i) {
-                for (int a = 0; a < 3; ++a) {
-                    smn[i][a] = fminf(smn[i + 1][a], unord(b[i].mn[a]));
-                    smx[i][a] = fmaxf(smx[i + 1][a], unord(b[i].mx[a]));
-                }
-                sc[i] = sc[i + 1] + b[i].count;
-            }
-            float best_cost = FLT_MAX;
-            const float sa_parent = sah_area(tk.mn, tk.mx);
-            for (int i = 1; i < kSahBuckets; ++i) {
-                const int nL = pc[i], nR = sc[i];
-                if (nL == 0 || nR == 0) continue;
-                const float sa_l = sah_area(pmn[i], pmx[i]);
-                const float sa_r = sah_area(smn[i], smx[i]);
-                const float cost =
-                    1.0f + ((float)nL * sa_l + (float)nR * sa_r) / (sa_parent > 0 ? sa_parent : 1.0f);
-                if (cost < best_cost) {
-                    best_cost = cost;
-                    c.best = i;
-                }
-            }
-            if (c.best >= 0) {
-                c.mode = 0;
-                c.nl = pc[c.best];
-                for (int a = 0; a < 3; ++a) {
-                    c.lmn[a] = pmn[c.best][a];
-                    c.lmx[a] = pmx[c.best][a];
-                    c.rmn[a] = smn[c.best][a];
-                    c.rmx[a] = smx[c.best][a];
-                }
-            }
+        float best_cost = FLT_MAX;
+        const float sa_parent = sah_area(tk.mn, tk.mx);
+        const SahBin* b = bins + (size_t)t * NB;
+        if constexpr (Q) {
+            for (int ax = 0; ax < 3; ++ax)
+                if (unord(cb[6 * t + 3 + ax]) > unord(cb[6 * t + ax]))
+                    sah_best_boundary(b + ax * kQualBuckets, kQualBuckets, ax, sa_parent, c,
+                                      best_cost);
+            if (c.mode == 1) c.axis = sah_axis(tk.mn, tk.mx);
+        } else {
+            if (tk.mx[c.axis] > tk.mn[c.axis])
+                sah_best_boundary(b, kSahBuckets, c.axis, sa_parent, c, best_cost);
         }
         ch[t] = c;
         if (c.mode == 1) fb_list[atomicAdd(n_fb, 1)] = t;
@@ -480,9 +571,11 @@ __global__ void sah_choose(const SahTask* tasks, int T, const SahBin* bins, SahC
 }
 
 // Stable partition of bucket-split tasks, pass 1: left-side count of each item.
+template <bool Q>
 __global__ void __launch_bounds__(kSahBlock)
 sah_part_count(const SahTask* tasks, int T, const int* item_off, const int* nchunk,
-               const SahChoice* ch, const int* perm, const DBox* boxes, int* left_cnt) {
+               const SahChoice* ch, const int* perm, const DBox* boxes, const int* cb,
+               int* left_cnt) {
     __shared__ int s_sum[kSahBlock / 32];
     const int items = item_off[T - 1] + nchunk[T - 1];
     if ((int)blockIdx.x >= items) return;
@@ -491,11 +584,10 @@ sah_part_count(const SahTask* tasks, int T, const int* item_off, const int* nchu
     const SahChoice c = ch[t];
     int cnt = 0;
     if (c.mode == 0) {
-        const float lo = tk.mn[c.axis], hi = tk.mx[c.axis];
         const int begin = tk.start + (blockIdx.x - item_off[t]) * kSahChunk;
         const int end = min(begin + kSahChunk, tk.start + tk.count);
         for (int p = begin + threadIdx.x; p < end; p += blockDim.x)
-            cnt += sah_bucket(boxes[perm[p]], c.axis, lo, hi) < c.best ? 1 : 0;
+            cnt += task_bucket<Q>(boxes[perm[p]], c.axis, tk, cb + 6 * t) < c.best ? 1 : 0;
     }
     for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
     if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = cnt;
@@ -509,10 +601,11 @@ sah_part_count(const SahTask* tasks, int T, const int* item_off, const int* nchu
 
 // Pass 2: every primitive of a bucket-split task to its place in `out`, the
 // left side first, each side in the order of `perm`.
+template <bool Q>
 __global__ void __launch_bounds__(kSahBlock)
 sah_part_write(const SahTask* tasks, int T, const int* item_off, const int* nchunk,
-               const SahChoice* ch, const int* perm, const DBox* boxes, const int* left_off,
-               int* out) {
+               const SahChoice* ch, const int* perm, const DBox* boxes, const int* cb,
+               const int* left_off, int* out) {
     __shared__ int s_warp[kSahBlock / 32];
     const int items = item_off[T - 1] + nchunk[T - 1];
     if ((int)blockIdx.x >= items) return;
@@ -520,7 +613,6 @@ sah_part_write(const SahTask* tasks, int T, const int* item_off, const int* nchu
     const SahTask tk = tasks[t];
     const SahChoice c = ch[t];
     if (c.mode != 0) return;
-    const float lo = tk.mn[c.axis], hi = tk.mx[c.axis];
     const int first_item = item_off[t];
     const int chunk0 = tk.start + (blockIdx.x - first_item) * kSahChunk;
     const int end = min(chunk0 + kSahChunk, tk.start + tk.count);
@@ -532,7 +624,7 @@ sah_part_write(const SahTask* tasks, int T, const int* item_off, const int* nchu
         const int p = p0 + threadIdx.x;
         const bool on = p < end;
         const int prim = on ? perm[p] : 0;
-        const bool left = on && sah_bucket(boxes[prim], c.axis, lo, hi) < c.best;
+        const bool left = on && task_bucket<Q>(boxes[prim], c.axis, tk, cb + 6 * t) < c.best;
         const unsigned m = __ballot_sync(0xffffffffu, left);
         if (lane == 0) s_warp[warp] = __popc(m);
         __syncthreads();
@@ -833,8 +925,10 @@ cudaError_t device_lbvh(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, 
 
 // Pencil's binned SAH tree, built on the current device; n_unified >= 2.
 // Device memory for the build is allocated here and freed before returning.
-cudaError_t device_sah(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, int& depth,
-                       cudaStream_t st, cudaMemPool_t pool) {
+template <bool Q>
+static cudaError_t device_sah_impl(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out,
+                                   int& depth, cudaStream_t st, cudaMemPool_t pool) {
+    constexpr int NB = kBinsPerTask<Q>;
     const int n = n_unified;
     const size_t np = (size_t)s.n_prims, nv = (size_t)s.n_mesh_vertices,
                  nt = (size_t)s.n_mesh_triangles;
@@ -853,7 +947,7 @@ cudaError_t device_sah(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, i
     size_t bytes = al(np * sizeof(pgpu_prim)) + al(nv * 12) + al(nt * 12) +
                    al((size_t)n * sizeof(DBox)) + 2 * al((size_t)n * 4) + al(8 * 4) +
                    2 * al((size_t)t_max * sizeof(SahTask)) + al((size_t)small_max * sizeof(SahSmall)) +
-                   al((size_t)t_max * kSahBuckets * sizeof(SahBin)) +
+                   al((size_t)t_max * NB * sizeof(SahBin)) + al((size_t)t_max * 6 * 4) +
                    al((size_t)t_max * sizeof(SahChoice)) + 2 * al((size_t)t_max * 4) +
                    2 * al((size_t)item_max * 4) + 3 * al((size_t)t_max * 4) +
                    2 * al((size_t)n * 4) + 2 * al((size_t)n * 4) +
@@ -873,7 +967,8 @@ cudaError_t device_sah(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, i
     SahTask* d_task[2] = {reinterpret_cast<SahTask*>(take((size_t)t_max * sizeof(SahTask))),
                           reinterpret_cast<SahTask*>(take((size_t)t_max * sizeof(SahTask)))};
     auto* d_small = reinterpret_cast<SahSmall*>(take((size_t)small_max * sizeof(SahSmall)));
-    auto* d_bins = reinterpret_cast<SahBin*>(take((size_t)t_max * kSahBuckets * sizeof(SahBin)));
+    auto* d_bins = reinterpret_cast<SahBin*>(take((size_t)t_max * NB * sizeof(SahBin)));
+    auto* d_cb = reinterpret_cast<int*>(take((size_t)t_max * 6 * 4));   // quality: centroid bounds
     auto* d_ch = reinterpret_cast<SahChoice*>(take((size_t)t_max * sizeof(SahChoice)));
     auto* d_nchunk = reinterpret_cast<int*>(take((size_t)t_max * 4));
     auto* d_item_off = reinterpret_cast<int*>(take((size_t)t_max * 4));
@@ -921,20 +1016,25 @@ cudaError_t device_sah(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, i
                                                st)) != cudaSuccess)
             return e;
         const int grid_items = std::min(item_max, T + n / kSahChunk + 1);
-        sah_bins_init<<<grid(T * kSahBuckets), B, 0, st>>>(d_bins, T * kSahBuckets);
-        sah_bin<<<grid_items, B, 0, st>>>(tasks, T, d_item_off, d_nchunk, d_perm, d_boxes,
-                                          d_bins);
+        if constexpr (Q) {
+            sah_cb_init<<<grid(T * 6), B, 0, st>>>(d_cb, T * 6);
+            sah_cbounds<<<grid_items, B, 0, st>>>(tasks, T, d_item_off, d_nchunk, d_perm,
+                                                  d_boxes, d_cb);
+        }
+        sah_bins_init<<<grid(T * NB), B, 0, st>>>(d_bins, T * NB);
+        sah_bin<Q><<<grid_items, B, 0, st>>>(tasks, T, d_item_off, d_nchunk, d_perm, d_boxes,
+                                             d_cb, d_bins);
         if ((e = cudaMemsetAsync(d_ctr + 6, 0, 2 * 4, st)) != cudaSuccess) return e;
-        sah_choose<<<grid(T), B, 0, st>>>(tasks, T, d_bins, d_ch, d_fb, d_ctr + 7);
+        sah_choose<Q><<<grid(T), B, 0, st>>>(tasks, T, d_bins, d_cb, d_ch, d_fb, d_ctr + 7);
         if ((e = cudaMemsetAsync(d_left_cnt, 0, (size_t)grid_items * 4, st)) != cudaSuccess)
             return e;
-        sah_part_count<<<grid_items, B, 0, st>>>(tasks, T, d_item_off, d_nchunk, d_ch, d_perm,
-                                                 d_boxes, d_left_cnt);
+        sah_part_count<Q><<<grid_items, B, 0, st>>>(tasks, T, d_item_off, d_nchunk, d_ch, d_perm,
+                                                    d_boxes, d_cb, d_left_cnt);
         if ((e = cub::DeviceScan::ExclusiveSum(d_scan_tmp, scan_bytes, d_left_cnt, d_left_off,
                                                grid_items, st)) != cudaSuccess)
             return e;
-        sah_part_write<<<grid_items, B, 0, st>>>(tasks, T, d_item_off, d_nchunk, d_ch, d_perm,
-                                                 d_boxes, d_left_off, d_tmp);
+        sah_part_write<Q><<<grid_items, B, 0, st>>>(tasks, T, d_item_off, d_nchunk, d_ch, d_perm,
+                                                    d_boxes, d_cb, d_left_off, d_tmp);
         sah_part_copy<<<grid_items, B, 0, st>>>(tasks, T, d_item_off, d_nchunk, d_ch, d_tmp,
                                                 d_perm);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -994,6 +1094,12 @@ cudaError_t device_sah(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, i
     if ((e = cudaMemcpyAsync(&depth, d_misc + 1, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return e;
     return cudaStreamSynchronize(st);
+}
+
+cudaError_t device_sah(const pgpu_scene& s, int n_unified, pgpu_bvh_node* out, int& depth,
+                       cudaStream_t st, cudaMemPool_t pool, bool quality) {
+    return quality ? device_sah_impl<true>(s, n_unified, out, depth, st, pool)
+                   : device_sah_impl<false>(s, n_unified, out, depth, st, pool);
 }
 
 }  // namespace pgpu

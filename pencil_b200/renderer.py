@@ -143,8 +143,10 @@ class GpuContext:
 
     def set_traversal_tree(self, mode: int) -> None:
         """Tree the wide traversals of later uploads walk:
-        A.TRAVERSAL_UPLOADED (the uploaded tree, default) or A.TRAVERSAL_LBVH
-        (a linear BVH over the uploaded leaves, built on the device)."""
+        A.TRAVERSAL_UPLOADED (the uploaded tree, default), A.TRAVERSAL_LBVH
+        (a linear BVH over the uploaded leaves, built on the device) or
+        A.TRAVERSAL_SAH (a 3-axis binned SAH tree over them, built on the
+        device)."""
         self.check(self.lib.pgpu_set_traversal_tree(self.h, int(mode)),
                    "pgpu_set_traversal_tree")
 

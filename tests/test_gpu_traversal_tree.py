@@ -1,5 +1,6 @@
-"""pgpu_set_traversal_tree: the wide traversals walk a linear BVH built on
-the device over the uploaded tree's leaves instead of the uploaded tree.
+"""pgpu_set_traversal_tree: the wide traversals walk a tree built on the
+device over the uploaded tree's leaves -- a linear BVH, or a binned SAH tree
+over centroid bounds on three axes -- instead of the uploaded tree.
 
 The leaves keep the uploaded tree's boxes and slots (its DFS leaf order,
 which decides among hits at equal distance as BVHNode::hit does,
@@ -21,10 +22,13 @@ from pencil_b200.renderer import RenderSettings
 pytestmark = pytest.mark.gpu
 
 
-def upload_both(gpu, scene, nodes=None):
-    """The scene uploaded twice: on the uploaded tree and on the LBVH."""
+MODES = [A.TRAVERSAL_LBVH, A.TRAVERSAL_SAH]
+
+
+def upload_both(gpu, scene, nodes=None, mode=A.TRAVERSAL_LBVH):
+    """The scene uploaded twice: on the uploaded tree and on a device tree."""
     a = gpu.upload(scene, nodes)
-    gpu.set_traversal_tree(A.TRAVERSAL_LBVH)
+    gpu.set_traversal_tree(mode)
     try:
         b = gpu.upload(scene, nodes)
     finally:
@@ -36,10 +40,11 @@ def same_pixels(x, y) -> float:
     return float(np.all(x.view(np.uint32) == y.view(np.uint32), axis=2).mean())
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name", GOLDEN_SCENES)
-def test_lbvh_traversal_finds_the_same_hits(gpu, name):
+def test_device_traversal_tree_finds_the_same_hits(gpu, name, mode):
     scene, fx = load_golden(name)
-    a, b = upload_both(gpu, scene, fx["nodes"])
+    a, b = upload_both(gpu, scene, fx["nodes"], mode)
     ia, ib = gpu.scene_info(a), gpu.scene_info(b)
     assert ia["n_leaves"] == ib["n_leaves"] and ia["bvh_depth"] == ib["bvh_depth"]
     uv = np.random.default_rng(11).uniform(0, 1, (20000, 2)).astype(np.float32)
@@ -55,29 +60,31 @@ def test_lbvh_traversal_finds_the_same_hits(gpu, name):
     gpu.free(b)
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name,engine", [("cornell_box", A.ENGINE_WAVEFRONT),
                                          ("cloud2k", A.ENGINE_WAVEFRONT),
                                          ("prims_mix", A.ENGINE_MEGAKERNEL),
                                          ("cloud2k", A.ENGINE_MEGAKERNEL)])
-def test_lbvh_traversal_renders_the_same_image(gpu, name, engine):
+def test_device_traversal_tree_renders_the_same_image(gpu, name, engine, mode):
     scene, fx = load_golden(name)
     wd, ht, _, depth = (int(x) for x in fx["settings"])
     st = RenderSettings(width=wd, height=ht, samples=4, max_depth=depth, pathtrace=True,
                         pathtrace_bounces=depth, engine=engine)
-    a, b = upload_both(gpu, scene, fx["nodes"])
+    a, b = upload_both(gpu, scene, fx["nodes"], mode)
     assert same_pixels(gpu.render(a, st), gpu.render(b, st)) >= 0.999
     gpu.free(a)
     gpu.free(b)
 
 
-def test_lbvh_traversal_on_the_full_mesh(gpu):
-    """The 1,310,720-triangle mesh box, the workload the mode is for: the
+@pytest.mark.parametrize("mode", MODES)
+def test_device_traversal_tree_on_the_full_mesh(gpu, mode):
+    """The 1,310,720-triangle mesh box, the workload the modes are for: the
     same hit distances for 50,000 camera rays, a window of the frame equal
     pixel for pixel but for rounding ties, fewer node visits per ray."""
     from pencil_b200.renderer import RenderStats
     w = W.mesh_box()
     nodes, _ = w.scene.build_bvh()
-    a, b = upload_both(gpu, w.scene, nodes)
+    a, b = upload_both(gpu, w.scene, nodes, mode)
     uv = np.random.default_rng(9).uniform(0, 1, (50000, 2)).astype(np.float32)
     pa, ta = gpu.primary_hits(a, uv)
     pb, tb = gpu.primary_hits(b, uv)
@@ -93,8 +100,8 @@ def test_lbvh_traversal_on_the_full_mesh(gpu):
         imgs.append(gpu.render_window(sid, st, win, stats=cnt))
         st.count_rays, st.count_nodes = False, False
         visits.append(cnt.ext_node_visits / max(1, cnt.extension_rays))
-    print(f"mesh window: {same_pixels(*imgs):.6f} of pixels equal; wide-node visits per "
-          f"extension ray {visits[0]:.1f} (uploaded tree) vs {visits[1]:.1f} (LBVH)")
+    print(f"mesh window, mode {mode}: {same_pixels(*imgs):.6f} of pixels equal; wide-node "
+          f"visits per extension ray {visits[0]:.1f} (uploaded tree) vs {visits[1]:.1f}")
     assert same_pixels(*imgs) >= 0.999
     assert visits[1] < visits[0]
     gpu.free(a)
@@ -102,5 +109,5 @@ def test_lbvh_traversal_on_the_full_mesh(gpu):
 
 
 def test_traversal_tree_rejects_unknown_modes(gpu):
-    assert gpu.lib.pgpu_set_traversal_tree(gpu.h, 2) == A.ERR_INVALID_ARG
+    assert gpu.lib.pgpu_set_traversal_tree(gpu.h, 3) == A.ERR_INVALID_ARG
     assert gpu.lib.pgpu_set_traversal_tree(gpu.h, -1) == A.ERR_INVALID_ARG
