@@ -200,6 +200,19 @@ inline int render(const pencil::ParsedScene& ps, const pencil::RenderSettings& r
     pgpu_ctx* ctx = nullptr;
     int rc = pgpu_create(device, &ctx);
     if (rc) { why = "no usable CUDA device"; return rc; }
+    // Scenes with a triangle mesh: the wide traversals walk a tree built on
+    // the device over Pencil's leaves (same leaf boxes and leaf order, so
+    // the same hits); Pencil's split binning over parent boxes groups a fine
+    // mesh inside large walls badly. PENCIL_GPU_TREE=uploaded|lbvh|sah
+    // chooses explicitly.
+    int tree = t.desc.n_mesh_triangles > 0 ? PGPU_TRAVERSAL_LBVH : PGPU_TRAVERSAL_UPLOADED;
+    if (const char* e = std::getenv("PENCIL_GPU_TREE")) {
+        const std::string v = e;
+        if (v == "uploaded") tree = PGPU_TRAVERSAL_UPLOADED;
+        else if (v == "lbvh") tree = PGPU_TRAVERSAL_LBVH;
+        else if (v == "sah") tree = PGPU_TRAVERSAL_SAH;
+    }
+    pgpu_set_traversal_tree(ctx, tree);
     int sid = 0;
     rc = pgpu_upload_scene(ctx, &t.desc, &sid);
     if (rc == PGPU_OK) {
