@@ -295,8 +295,13 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
 // between node steps; when few lanes of the warp are still busy, the idle
 // lanes take new rays from the queue (one atomic per warp), so warps keep
 // traversing instead of waiting for their slowest ray.
+// Resident blocks of kWfMaxBlock threads the register allocation of the
+// extension kernel must allow (1: the compiler's choice, 72 registers).
+#ifndef PGPU_EXTEND_MIN_BLOCKS
+#define PGPU_EXTEND_MIN_BLOCKS 1
+#endif
 template <bool COUNT, bool ONE>
-__global__ void __launch_bounds__(kWfMaxBlock)
+__global__ void __launch_bounds__(kWfMaxBlock, PGPU_EXTEND_MIN_BLOCKS)
 wf_extend(WfArgs A, int it) {
     extern __shared__ int smem[];
     TravStack<kWfShared> stk;
@@ -718,7 +723,10 @@ wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
 // At most 80 registers (three blocks of 256 or six of 128 threads per SM):
 // left free the kernel takes 105 (127 with 8-wide nodes), which leaves four
 // blocks of 128 per SM -- too few warps to hide the latency of its loads.
-constexpr int kShadowMinBlocks = 3;
+#ifndef PGPU_SHADOW_MIN_BLOCKS
+#define PGPU_SHADOW_MIN_BLOCKS 3
+#endif
+constexpr int kShadowMinBlocks = PGPU_SHADOW_MIN_BLOCKS;
 
 template <bool COUNT, bool ONE>
 __global__ void __launch_bounds__(kWfMaxBlock, kShadowMinBlocks)
