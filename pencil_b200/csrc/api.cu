@@ -923,6 +923,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     v.n_lights = s->n_lights;
     v.n_leaves = n_leaf;
     v.has_quad_lights = has_quad;
+    v.has_glass = has_glass ? 1 : 0;
     if (n_nodes == 0) {
         v.root_ref = kEmptyRoot;
     } else {
@@ -1040,6 +1041,7 @@ int32_t pgpu_update_materials(pgpu_ctx* c, int32_t id, const pgpu_material* m, i
                                  cudaMemcpyHostToDevice, c->stream));
     PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     ds->has_glass = has_glass;
+    ds->view.has_glass = has_glass ? 1 : 0;
     return PGPU_OK;
 }
 
