@@ -333,30 +333,64 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     }
     // DFS pre-order (the order Pencil's recursive build emits): an interior
     // node k has its left subtree at k + 1 and its right subtree right after
-    // the left one. Subtree sizes, from the back, check exactly that; the
-    // same sweep takes subtree heights (the root's is the depth), checks
-    // that every primitive is in exactly one leaf and numbers the interior
-    // nodes and the leaves in DFS order (c->ws_idx; counted from the back,
-    // as a valid table has n_prims leaves and n_prims - 1 interior nodes).
+    // the left one. On the host threads, per chunk of the table: every leaf
+    // names a primitive in range, and no primitive is in two leaves; the
+    // leaves and interior nodes are counted, so that a node's DFS number
+    // (c->ws_idx) is the count of its kind before it. Then one sweep from
+    // the back takes subtree sizes, which check the pre-order exactly, and
+    // heights (the root's is the depth).
     std::vector<int2>& sh = c->ws_size_height;     // (subtree size, height)
     sh.resize(n_nodes);
     std::vector<int>& idx = c->ws_idx;
     idx.resize(n_nodes);
     std::vector<char>& seen = c->ws_seen;
     seen.assign(n_prims, 0);
-    int next_leaf = n_prims - 1, next_int = n_prims - 2;
+    const int T = std::max(1, std::min(host_threads(), (n_nodes + 16383) / 16384));
+    const int chunk = (n_nodes + T - 1) / T;
+    std::vector<int> leaves_before(T + 1, 0);
+    std::atomic<int> bad_range{n_nodes}, bad_twice{n_nodes};
+    auto lower = [](std::atomic<int>& a, int k) {
+        int cur = a.load();
+        while (k < cur && !a.compare_exchange_weak(cur, k)) {}
+    };
+    auto leaves_pass = [&](int t) {
+        const int b = t * chunk, e = std::min(n_nodes, b + chunk);
+        int cnt = 0;
+        for (int k = b; k < e; ++k) {
+            const pgpu_bvh_node& nd = nodes[k];
+            if (nd.left >= 0) continue;
+            ++cnt;
+            if (nd.right < 0 || nd.right >= n_prims) { lower(bad_range, k); continue; }
+            if (__atomic_exchange_n(&seen[nd.right], (char)1, __ATOMIC_RELAXED)) lower(bad_twice, k);
+        }
+        leaves_before[t + 1] = cnt;
+    };
+    if (T > 1) host_run(T, leaves_pass);
+    else leaves_pass(0);
+    if (bad_range.load() < n_nodes) {
+        const int k = bad_range.load();
+        return fail(c, PGPU_ERR_BVH_INVALID, "leaf %d references primitive %d", k, nodes[k].right);
+    }
+    if (bad_twice.load() < n_nodes)
+        return fail(c, PGPU_ERR_BVH_INVALID, "primitive %d is in two leaves",
+                    nodes[bad_twice.load()].right);
+    for (int t = 0; t < T; ++t) leaves_before[t + 1] += leaves_before[t];
+    if (leaves_before[T] != n_prims)
+        return fail(c, PGPU_ERR_BVH_INVALID, "%d leaves for %d primitives", leaves_before[T],
+                    n_prims);
+    auto number_pass = [&](int t) {
+        const int b = t * chunk, e = std::min(n_nodes, b + chunk);
+        int leaf = leaves_before[t], inner = b - leaves_before[t];
+        for (int k = b; k < e; ++k) idx[k] = nodes[k].left < 0 ? leaf++ : inner++;
+    };
+    if (T > 1) host_run(T, number_pass);
+    else number_pass(0);
     for (int k = n_nodes - 1; k >= 0; --k) {
         const pgpu_bvh_node& nd = nodes[k];
         if (nd.left < 0) {
-            if (nd.right < 0 || nd.right >= n_prims)
-                return fail(c, PGPU_ERR_BVH_INVALID, "leaf %d references primitive %d", k, nd.right);
-            if (seen[nd.right]++)
-                return fail(c, PGPU_ERR_BVH_INVALID, "primitive %d is in two leaves", nd.right);
             sh[k] = make_int2(1, 1);
-            idx[k] = next_leaf--;
             continue;
         }
-        idx[k] = next_int--;
         if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes ||
             nd.right != nd.left + sh[nd.left].x)
             return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
@@ -923,7 +957,6 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     v.n_lights = s->n_lights;
     v.n_leaves = n_leaf;
     v.has_quad_lights = has_quad;
-    v.has_glass = has_glass ? 1 : 0;
     if (n_nodes == 0) {
         v.root_ref = kEmptyRoot;
     } else {
@@ -1041,7 +1074,6 @@ int32_t pgpu_update_materials(pgpu_ctx* c, int32_t id, const pgpu_material* m, i
                                  cudaMemcpyHostToDevice, c->stream));
     PGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     ds->has_glass = has_glass;
-    ds->view.has_glass = has_glass ? 1 : 0;
     return PGPU_OK;
 }
 

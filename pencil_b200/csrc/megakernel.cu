@@ -18,10 +18,7 @@ namespace pgpu {
 
 constexpr int kMkShared = 16;   // stack entries per thread kept in shared memory
 
-// LEAN: path tracing over a scene without dielectrics (the shading state
-// machine without its Whitted and glass branches, as the wavefront's shade
-// kernel runs it for such frames).
-template <bool COUNT, bool TREE, bool PIXEL_SEQ, bool WIDE, bool LEAN = false>
+template <bool COUNT, bool TREE, bool PIXEL_SEQ, bool WIDE>
 __global__ void __launch_bounds__(128)
 mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __restrict__ m2,
           unsigned long long* __restrict__ counters) {
@@ -31,7 +28,7 @@ mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __re
     stk.st = reinterpret_cast<float*>(smem + kMkShared * blockDim.x) + threadIdx.x;
     stk.stride = blockDim.x;
     RayCount rc = {};
-    Tracer<kMkShared, COUNT, WIDE, LEAN> tr{S, P, stk, rc};
+    Tracer<kMkShared, COUNT, WIDE> tr{S, P, stk, rc};
 
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool tile = P.tile_w > 0;
@@ -98,15 +95,15 @@ mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __re
     }
 }
 
-template <bool COUNT, bool TREE, bool PIXEL_SEQ, bool WIDE, bool LEAN = false>
+template <bool COUNT, bool TREE, bool PIXEL_SEQ, bool WIDE>
 static cudaError_t launch_mk(const SceneView& S, const PathParams& P, int G, float* out,
                              float* m2, unsigned long long* counters, cudaStream_t st) {
     const int block = 128;
     long long threads = (P.tile_w > 0 ? (long long)P.tile_w * P.tile_h : (long long)P.W * P.H) * G;
     long long blocks = (threads + block - 1) / block;
     size_t smem = (size_t)kMkShared * block * 8;
-    mk_render<COUNT, TREE, PIXEL_SEQ, WIDE, LEAN><<<(unsigned)blocks, block, smem, st>>>(
-        S, P, G, out, m2, counters);
+    mk_render<COUNT, TREE, PIXEL_SEQ, WIDE><<<(unsigned)blocks, block, smem, st>>>(S, P, G, out,
+                                                                                     m2, counters);
     return cudaGetLastError();
 }
 
@@ -123,12 +120,6 @@ cudaError_t launch_megakernel(const SceneView& S, const RenderCfg& c, float* out
         while (G * 2 <= lim) G *= 2;
     }
     const bool wide = !c.binary_tree;
-    // the production path (counter RNG, Fresnel-split glass, wide tree) over
-    // a scene without dielectrics takes the lean shading variant, as the
-    // wavefront does
-    if (wide && !tree && !seq && c.mode == PGPU_MODE_PATHTRACE && !S.has_glass)
-        return c.count ? launch_mk<true, false, false, true, true>(S, P, G, out, m2, counters, st)
-                       : launch_mk<false, false, false, true, true>(S, P, G, out, m2, counters, st);
 #define PGPU_MK_CASE(CNT, TR, SQ)                                                \
     if (c.count == CNT && tree == TR && seq == SQ)                               \
         return wide ? launch_mk<CNT, TR, SQ, true>(S, P, G, out, m2, counters, st) \

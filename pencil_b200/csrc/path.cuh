@@ -222,13 +222,10 @@ struct NeeAccum {
 // continues with ps.ray. Semantics: trace_path (src/renderer.hpp:829-972)
 // and, after glass, trace (src/renderer.hpp:403-822) followed along the
 // Fresnel-chosen branch of trace_dielectric (src/renderer.hpp:1582-1627).
-// LEAN: a path-trace frame over scenes without dielectrics, where no vertex
-// is a Whitted vertex and none is glass: the same arithmetic with those
-// branches compiled out (a smaller shading kernel).
-template <class Emit, bool LEAN = false>
+template <class Emit>
 __device__ __forceinline__ bool shade_vertex(const SceneView& S, const PathParams& P,
                                              PathState& ps, bool found, const Hit& h, Emit& E) {
-    const bool whitted = !LEAN && (ps.flags & kFlagWhitted) != 0;
+    const bool whitted = (ps.flags & kFlagWhitted) != 0;
     if (!found) {
         ps.L = ps.L + ps.T * ld3(S.bg);
         return false;
@@ -236,7 +233,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& S, const PathParam
     const DevMaterial& m = S.mats[h.mat];
     const V3 albedo = ld3(m.albedo);
     const bool metal = m.kind == 1 && m.reflectivity > 0.0f;
-    const bool glass = !LEAN && m.kind == 2;
+    const bool glass = m.kind == 2;
     const V3 sorg = h.p + h.n * P.bias;
     if (!whitted) {
         const bool diffuse = !metal && !glass;
@@ -335,9 +332,8 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& S, const PathParam
 // One path traced to the end by one thread (megakernel). WIDE: traversal of
 // the 4-wide tree the wavefront walks (ClosestTrav4/AnyTrav4); otherwise
 // Pencil's binary tree (the tree BVHNode::hit walks, src/bvh.hpp:31-48) in
-// its child-pair layout, nearest child first. LEAN: shade_vertex's lean
-// variant (path tracing over a scene without dielectrics).
-template <int kShared, bool COUNT, bool WIDE = false, bool LEAN = false>
+// its child-pair layout, nearest child first.
+template <int kShared, bool COUNT, bool WIDE = false>
 struct Tracer {
     const SceneView& S;
     const PathParams& P;
@@ -581,7 +577,7 @@ struct Tracer {
             Hit h;
             bool found = closest(ps.ray, h) >= 0;
             InlineNee emit{*this};
-            alive = shade_vertex<InlineNee, LEAN>(S, P, ps, found, h, emit);
+            alive = shade_vertex(S, P, ps, found, h, emit);
             emit.acc.finish(ps.L, emit.tail, emit.w, emit.s);
             if (COUNT && alive && (ps.flags & kFlagWhitted)) rc.ref++;
         }

@@ -119,7 +119,6 @@ struct SceneView {
     int n_leaves;
     int root_ref;          // ref of the root (interior 0, a leaf ref, or kEmpty)
     int has_quad_lights;
-    int has_glass;         // a dielectric material: path-trace vertices can turn Whitted
     float root_min[3];
     float root_max[3];
     float cam[21];         // origin, lower_left, horizontal, vertical, u, v, w

@@ -295,13 +295,8 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
 // between node steps; when few lanes of the warp are still busy, the idle
 // lanes take new rays from the queue (one atomic per warp), so warps keep
 // traversing instead of waiting for their slowest ray.
-// Resident blocks of kWfMaxBlock threads the register allocation of the
-// extension kernel must allow (1: the compiler's choice, 72 registers).
-#ifndef PGPU_EXTEND_MIN_BLOCKS
-#define PGPU_EXTEND_MIN_BLOCKS 1
-#endif
 template <bool COUNT, bool ONE>
-__global__ void __launch_bounds__(kWfMaxBlock, PGPU_EXTEND_MIN_BLOCKS)
+__global__ void __launch_bounds__(kWfMaxBlock)
 wf_extend(WfArgs A, int it) {
     extern __shared__ int smem[];
     TravStack<kWfShared> stk;
@@ -536,9 +531,7 @@ struct StoreNee {
 
 // At most 72 registers (28 warps per SM): the shading state machine is
 // latency-bound, and the extra resident warps pay for a few spilled words.
-// LEAN: every job traces paths (not Whitted) over a scene without
-// dielectrics (shade_vertex<.., true>: no Whitted or glass branches).
-template <bool COUNT, bool ONE, bool LEAN>
+template <bool COUNT, bool ONE>
 __global__ void __maxnreg__(72)
 wf_shade(WfArgs A, int it) {
     RayCount rc = {};
@@ -576,7 +569,7 @@ wf_shade(WfArgs A, int it) {
             bool found = leaf >= 0;
             if (found) make_hit(S, __float_as_int(hv.y), leaf, ps.ray, 1e-4f, hv.x, h);
             StoreNee E(A, slot);
-            alive = shade_vertex<StoreNee, LEAN>(S, J.P, ps, found, h, E);
+            alive = shade_vertex(S, J.P, ps, found, h, E);
             E.store();
             shadow_work = E.kind != 0;
             if (A.sort_key >= 2 && shadow_work) key = sort_key_of(S, E.o0, E.d0);
@@ -725,10 +718,7 @@ wf_sort_scatter(const int* list, const int* count, const int* keyof, int* hist,
 // At most 80 registers (three blocks of 256 or six of 128 threads per SM):
 // left free the kernel takes 105 (127 with 8-wide nodes), which leaves four
 // blocks of 128 per SM -- too few warps to hide the latency of its loads.
-#ifndef PGPU_SHADOW_MIN_BLOCKS
-#define PGPU_SHADOW_MIN_BLOCKS 3
-#endif
-constexpr int kShadowMinBlocks = PGPU_SHADOW_MIN_BLOCKS;
+constexpr int kShadowMinBlocks = 3;
 
 template <bool COUNT, bool ONE>
 __global__ void __launch_bounds__(kWfMaxBlock, kShadowMinBlocks)
@@ -1029,22 +1019,15 @@ struct WfOccupancy {
     int grid_accumulate = 0;
 };
 
-// Resident blocks of the shading kernel per SM, for the variant a frame runs.
 template <bool COUNT, bool ONE>
-static cudaError_t shade_blocks(int& b, int blk, bool lean) {
-    return lean ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, wf_shade<COUNT, ONE, true>, blk, 0)
-                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, wf_shade<COUNT, ONE, false>, blk, 0);
-}
-
-template <bool COUNT, bool ONE>
-static cudaError_t occupancy(WfOccupancy& o, int blk = kWfBlock, bool lean = false) {
+static cudaError_t occupancy(WfOccupancy& o, int blk = kWfBlock) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     size_t smem = (size_t)kWfShared * blk * 8;
     int b1 = 0, b2 = 0, b3 = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, wf_extend<COUNT, ONE>, blk, smem);
-    if (e == cudaSuccess) e = shade_blocks<COUNT, ONE>(b2, blk, lean);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, wf_shade<COUNT, ONE>, blk, 0);
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, wf_shadow<COUNT, ONE>, blk, smem);
     o.grid_extend = sms * std::max(b1, 1);
     o.grid_shade = sms * std::max(b2, 1);
@@ -1089,11 +1072,10 @@ struct LaunchTimer {
 // ONE: a one-scene frame (W.args.view0 / job0 hold its scene and job).
 template <bool COUNT, bool ONE>
 static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& jobs, int iters,
-                                 int Qeff, bool lean, cudaStream_t st, int* launches,
-                                 LaunchTimer& lt) {
+                                 int Qeff, cudaStream_t st, int* launches, LaunchTimer& lt) {
     const int blk = W.block;
     WfOccupancy occ;
-    cudaError_t e = occupancy<COUNT, ONE>(occ, blk, lean);
+    cudaError_t e = occupancy<COUNT, ONE>(occ, blk);
     if (e != cudaSuccess) return e;
     const bool packet_first = ONE && W.args.packets != 0;
     // timed (profiled) frames stay on one stream so that kernel classes add
@@ -1160,8 +1142,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
             if (sort_next &&
                 (e = cudaMemsetAsync(A.hist_e, 0, (size_t)kSortBinsE * 4, st)) != cudaSuccess)
                 return e;
-            if (lean) wf_shade<COUNT, ONE, true><<<occ.grid_shade, blk, 0, st>>>(A, it);
-            else wf_shade<COUNT, ONE, false><<<occ.grid_shade, blk, 0, st>>>(A, it);
+            wf_shade<COUNT, ONE><<<occ.grid_shade, blk, 0, st>>>(A, it);
             if (A.sort_key >= 2) {
                 wf_sort_scan<<<kSortChunks, kSortChunk, 0, st>>>(A.hist_s, A.chunk_off);
                 wf_sort_chunks<kSortChunks><<<1, kSortChunk, 0, st>>>(A.chunk_off);
@@ -1269,10 +1250,6 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     W.args.maxS = maxS;
     W.block = block > 0 ? block : kWfBlock;
     const bool one = n == 1;
-    // the lean shading kernel when no vertex can be a Whitted or glass one
-    bool lean = true;
-    for (const RenderCfg& c : cfgs) lean = lean && c.mode == PGPU_MODE_PATHTRACE;
-    for (const SceneView& v : views) lean = lean && !v.has_glass;
     if (one) {
         W.args.view0 = views[jobs[0].view];
         W.args.job0 = jobs[0];
@@ -1308,7 +1285,6 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     }
     mix((unsigned long long)iters);
     mix((unsigned long long)one);
-    mix((unsigned long long)lean);
     // a one-scene graph also bakes the scene and job into its kernel
     // parameters: it is reused only while they are byte for byte the same
     const bool same_params =
@@ -1318,11 +1294,10 @@ cudaError_t wavefront_render(WfScratch& W, const std::vector<SceneView>& views,
     LaunchTimer lt;
     lt.on = kernel_ms != nullptr;
     auto enqueue = [&](int* nl_out) {
-        const int q = (int)Q;
-        return count ? (one ? enqueue_frame<true, true>(W, jobs, iters, q, lean, st, nl_out, lt)
-                            : enqueue_frame<true, false>(W, jobs, iters, q, lean, st, nl_out, lt))
-                     : (one ? enqueue_frame<false, true>(W, jobs, iters, q, lean, st, nl_out, lt)
-                            : enqueue_frame<false, false>(W, jobs, iters, q, lean, st, nl_out, lt));
+        return count ? (one ? enqueue_frame<true, true>(W, jobs, iters, (int)Q, st, nl_out, lt)
+                            : enqueue_frame<true, false>(W, jobs, iters, (int)Q, st, nl_out, lt))
+                     : (one ? enqueue_frame<false, true>(W, jobs, iters, (int)Q, st, nl_out, lt)
+                            : enqueue_frame<false, false>(W, jobs, iters, (int)Q, st, nl_out, lt));
     };
     if (lt.on) use_graph = false;
     // a frame shape met for the first time runs as direct launches: a graph
@@ -1569,7 +1544,7 @@ cudaError_t wavefront_render_static(int device, const SceneView& view, const Dev
             A, path0, (int)slots);
         for (int it = 0; it < c.depth; ++it) {
             wf_extend<false, true><<<occ.grid_extend, kWfBlock, smem, st>>>(A, it);
-            wf_shade<false, true, false><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
+            wf_shade<false, true><<<occ.grid_shade, kWfBlock, 0, st>>>(A, it);
             wf_shadow<false, true><<<occ.grid_shadow, kWfBlock, smem, st>>>(A, it);
         }
         wf_accumulate<<<accumulate_blocks(pixels, occ.grid_accumulate), kWfBlock, 0, st>>>(
