@@ -336,11 +336,14 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     // the left one. On the host threads, per chunk of the table: every leaf
     // names a primitive in range, and no primitive is in two leaves; the
     // leaves and interior nodes are counted, so that a node's DFS number
-    // (c->ws_idx) is the count of its kind before it. Then one sweep from
-    // the back takes subtree sizes, which check the pre-order exactly, and
-    // heights (the root's is the depth).
-    std::vector<int2>& sh = c->ws_size_height;     // (subtree size, height)
-    sh.resize(n_nodes);
+    // (c->ws_idx) is the count of its kind before it. Then one forward sweep
+    // walks the table as a pre-order traversal would, with a stack of the
+    // right children still to come (and their levels): an interior node's
+    // left child must come next, and after a leaf the innermost pending
+    // right child; nothing may be left pending. The deepest leaf's level is
+    // the depth.
+    std::vector<int2>& pending = c->ws_size_height;   // (right child, its level)
+    pending.clear();
     std::vector<int>& idx = c->ws_idx;
     idx.resize(n_nodes);
     std::vector<char>& seen = c->ws_seen;
@@ -385,20 +388,25 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     };
     if (T > 1) host_run(T, number_pass);
     else number_pass(0);
-    for (int k = n_nodes - 1; k >= 0; --k) {
+    int level = 1;
+    for (int k = 0; k < n_nodes; ++k) {
         const pgpu_bvh_node& nd = nodes[k];
-        if (nd.left < 0) {
-            sh[k] = make_int2(1, 1);
+        if (nd.left >= 0) {
+            if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes)
+                return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
+            pending.push_back(make_int2(nd.right, level + 1));
+            ++level;
             continue;
         }
-        if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes ||
-            nd.right != nd.left + sh[nd.left].x)
-            return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
-        sh[k] = make_int2(1 + sh[nd.left].x + sh[nd.right].x,
-                          1 + std::max(sh[nd.left].y, sh[nd.right].y));
+        depth = std::max(depth, level);
+        if (k + 1 == n_nodes) break;
+        if (pending.empty() || pending.back().x != k + 1)
+            return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k + 1);
+        level = pending.back().y;
+        pending.pop_back();
     }
-    if (sh[0].x != n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "unreachable nodes in table");
-    depth = sh[0].y;
+    if (!pending.empty() || nodes[n_nodes - 1].left >= 0)
+        return fail(c, PGPU_ERR_BVH_INVALID, "unreachable nodes in table");
     if (depth > kMaxDepth)
         return fail(c, PGPU_ERR_UNSUPPORTED, "BVH depth %d exceeds %d", depth, kMaxDepth);
     return PGPU_OK;
