@@ -821,8 +821,17 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         const float* v = s->mesh_vertices + 3 * (size_t)i;
         return make_float4(v[0], v[1], v[2], 0.0f);
     };
+    // the table is read in order, but a node's right child and a leaf's
+    // primitive lie anywhere: they are fetched a few nodes ahead
+    constexpr int kAhead = 16;
     auto convert = [&](int kb, int ke) {
     for (int k = kb; k < ke; ++k) {
+        if (k + kAhead < ke) {
+            const pgpu_bvh_node& f = nodes[k + kAhead];
+            if (f.left >= 0) __builtin_prefetch(&nodes[f.right]);
+            else if (f.right < s->n_prims) __builtin_prefetch(&s->prims[f.right]);
+            else __builtin_prefetch(&s->mesh_indices[3 * (size_t)(f.right - s->n_prims)]);
+        }
         const pgpu_bvh_node& nd = nodes[k];
         if (nd.left >= 0) {
             const pgpu_bvh_node& L = nodes[nd.left];
