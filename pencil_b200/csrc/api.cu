@@ -316,7 +316,15 @@ DevMaterial dev_material(const pgpu_material& m) {
     return d;
 }
 
-int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims, int& depth) {
+int check_preorder(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int& depth);
+
+// The uploaded table: finite boxes, links in range, leaves naming each
+// primitive once, DFS numbers of interior nodes and leaves (c->ws_idx). With
+// `order`, also the pre-order sweep (check_preorder); without, the caller
+// runs it (it is sequential) beside other work: what is checked here already
+// keeps every read of the table in range.
+int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims, int& depth,
+               bool order = true) {
     depth = 0;
     if (n_prims == 0) {
         if (n_nodes != 0) return fail(c, PGPU_ERR_BVH_INVALID, "nodes given for an empty scene");
@@ -336,14 +344,9 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     // the left one. On the host threads, per chunk of the table: every leaf
     // names a primitive in range, and no primitive is in two leaves; the
     // leaves and interior nodes are counted, so that a node's DFS number
-    // (c->ws_idx) is the count of its kind before it. Then one forward sweep
+    // (c->ws_idx) is the count of its kind before it. check_preorder then
     // walks the table as a pre-order traversal would, with a stack of the
-    // right children still to come (and their levels): an interior node's
-    // left child must come next, and after a leaf the innermost pending
-    // right child; nothing may be left pending. The deepest leaf's level is
-    // the depth.
-    std::vector<int2>& pending = c->ws_size_height;   // (right child, its level)
-    pending.clear();
+    // right children still to come (and their levels).
     std::vector<int>& idx = c->ws_idx;
     idx.resize(n_nodes);
     std::vector<char>& seen = c->ws_seen;
@@ -351,7 +354,7 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     const int T = std::max(1, std::min(host_threads(), (n_nodes + 16383) / 16384));
     const int chunk = (n_nodes + T - 1) / T;
     std::vector<int> leaves_before(T + 1, 0);
-    std::atomic<int> bad_range{n_nodes}, bad_twice{n_nodes};
+    std::atomic<int> bad_range{n_nodes}, bad_twice{n_nodes}, bad_link{n_nodes};
     auto lower = [](std::atomic<int>& a, int k) {
         int cur = a.load();
         while (k < cur && !a.compare_exchange_weak(cur, k)) {}
@@ -361,7 +364,11 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
         int cnt = 0;
         for (int k = b; k < e; ++k) {
             const pgpu_bvh_node& nd = nodes[k];
-            if (nd.left >= 0) continue;
+            if (nd.left >= 0) {
+                if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes)
+                    lower(bad_link, k);
+                continue;
+            }
             ++cnt;
             if (nd.right < 0 || nd.right >= n_prims) { lower(bad_range, k); continue; }
             if (__atomic_exchange_n(&seen[nd.right], (char)1, __ATOMIC_RELAXED)) lower(bad_twice, k);
@@ -370,6 +377,8 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     };
     if (T > 1) host_run(T, leaves_pass);
     else leaves_pass(0);
+    if (bad_link.load() < n_nodes)
+        return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", bad_link.load());
     if (bad_range.load() < n_nodes) {
         const int k = bad_range.load();
         return fail(c, PGPU_ERR_BVH_INVALID, "leaf %d references primitive %d", k, nodes[k].right);
@@ -388,6 +397,18 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     };
     if (T > 1) host_run(T, number_pass);
     else number_pass(0);
+    return order ? check_preorder(c, nodes, n_nodes, depth) : PGPU_OK;
+}
+
+// One forward sweep over a table whose links are in range (check_tree): an
+// interior node's left child must come next, and after a leaf the innermost
+// pending right child; nothing may be left pending. The deepest leaf's
+// level is the depth.
+int check_preorder(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int& depth) {
+    depth = 0;
+    if (n_nodes == 0) return PGPU_OK;
+    std::vector<int2>& pending = c->ws_size_height;   // (right child, its level)
+    pending.clear();
     int level = 1;
     for (int k = 0; k < n_nodes; ++k) {
         const pgpu_bvh_node& nd = nodes[k];
@@ -746,7 +767,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         nodes = built.data();
         n_nodes = (int)built.size();
     }
-    int rc = check_tree(c, nodes, n_nodes, nU, depth);
+    int rc = check_tree(c, nodes, n_nodes, nU, depth, /*order=*/false);
     if (rc) return rc;
 
     // DFS order numbering of interior nodes and leaf slots (check_tree)
@@ -884,7 +905,21 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         if (h_gc) h_gc[slot] = c;
     }
     };
-    parallel_for(n_nodes, convert);
+    // the sequential pre-order sweep runs beside the conversion, which reads
+    // nothing outside the table (its links are checked already)
+    {
+        const int C = std::max(1, std::min(4 * host_threads(), (n_nodes + 4095) / 4096));
+        const int chunk = (n_nodes + C - 1) / C;
+        host_run(C + 1, [&](int t) {
+            if (t == 0) {
+                rc = check_preorder(c, nodes, n_nodes, depth);
+                return;
+            }
+            const int b = (t - 1) * chunk, e = std::min(n_nodes, b + chunk);
+            if (b < e) convert(b, e);
+        });
+        if (rc) return rc;
+    }
 
     PGPU_CUDA(c, cudaSetDevice(c->device));
     auto ds = std::make_unique<DeviceScene>();
