@@ -316,15 +316,7 @@ DevMaterial dev_material(const pgpu_material& m) {
     return d;
 }
 
-int check_preorder(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int& depth);
-
-// The uploaded table: finite boxes, links in range, leaves naming each
-// primitive once, DFS numbers of interior nodes and leaves (c->ws_idx). With
-// `order`, also the pre-order sweep (check_preorder); without, the caller
-// runs it (it is sequential) beside other work: what is checked here already
-// keeps every read of the table in range.
-int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims, int& depth,
-               bool order = true) {
+int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims, int& depth) {
     depth = 0;
     if (n_prims == 0) {
         if (n_nodes != 0) return fail(c, PGPU_ERR_BVH_INVALID, "nodes given for an empty scene");
@@ -341,93 +333,38 @@ int check_tree(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int n_prims
     }
     // DFS pre-order (the order Pencil's recursive build emits): an interior
     // node k has its left subtree at k + 1 and its right subtree right after
-    // the left one. On the host threads, per chunk of the table: every leaf
-    // names a primitive in range, and no primitive is in two leaves; the
-    // leaves and interior nodes are counted, so that a node's DFS number
-    // (c->ws_idx) is the count of its kind before it. check_preorder then
-    // walks the table as a pre-order traversal would, with a stack of the
-    // right children still to come (and their levels).
+    // the left one. Subtree sizes, from the back, check exactly that; the
+    // same sweep takes subtree heights (the root's is the depth), checks
+    // that every primitive is in exactly one leaf and numbers the interior
+    // nodes and the leaves in DFS order (c->ws_idx; counted from the back,
+    // as a valid table has n_prims leaves and n_prims - 1 interior nodes).
+    std::vector<int2>& sh = c->ws_size_height;     // (subtree size, height)
+    sh.resize(n_nodes);
     std::vector<int>& idx = c->ws_idx;
     idx.resize(n_nodes);
     std::vector<char>& seen = c->ws_seen;
     seen.assign(n_prims, 0);
-    const int T = std::max(1, std::min(host_threads(), (n_nodes + 16383) / 16384));
-    const int chunk = (n_nodes + T - 1) / T;
-    std::vector<int> leaves_before(T + 1, 0);
-    std::atomic<int> bad_range{n_nodes}, bad_twice{n_nodes}, bad_link{n_nodes};
-    auto lower = [](std::atomic<int>& a, int k) {
-        int cur = a.load();
-        while (k < cur && !a.compare_exchange_weak(cur, k)) {}
-    };
-    auto leaves_pass = [&](int t) {
-        const int b = t * chunk, e = std::min(n_nodes, b + chunk);
-        int cnt = 0;
-        for (int k = b; k < e; ++k) {
-            const pgpu_bvh_node& nd = nodes[k];
-            if (nd.left >= 0) {
-                if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes)
-                    lower(bad_link, k);
-                continue;
-            }
-            ++cnt;
-            if (nd.right < 0 || nd.right >= n_prims) { lower(bad_range, k); continue; }
-            if (__atomic_exchange_n(&seen[nd.right], (char)1, __ATOMIC_RELAXED)) lower(bad_twice, k);
-        }
-        leaves_before[t + 1] = cnt;
-    };
-    if (T > 1) host_run(T, leaves_pass);
-    else leaves_pass(0);
-    if (bad_link.load() < n_nodes)
-        return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", bad_link.load());
-    if (bad_range.load() < n_nodes) {
-        const int k = bad_range.load();
-        return fail(c, PGPU_ERR_BVH_INVALID, "leaf %d references primitive %d", k, nodes[k].right);
-    }
-    if (bad_twice.load() < n_nodes)
-        return fail(c, PGPU_ERR_BVH_INVALID, "primitive %d is in two leaves",
-                    nodes[bad_twice.load()].right);
-    for (int t = 0; t < T; ++t) leaves_before[t + 1] += leaves_before[t];
-    if (leaves_before[T] != n_prims)
-        return fail(c, PGPU_ERR_BVH_INVALID, "%d leaves for %d primitives", leaves_before[T],
-                    n_prims);
-    auto number_pass = [&](int t) {
-        const int b = t * chunk, e = std::min(n_nodes, b + chunk);
-        int leaf = leaves_before[t], inner = b - leaves_before[t];
-        for (int k = b; k < e; ++k) idx[k] = nodes[k].left < 0 ? leaf++ : inner++;
-    };
-    if (T > 1) host_run(T, number_pass);
-    else number_pass(0);
-    return order ? check_preorder(c, nodes, n_nodes, depth) : PGPU_OK;
-}
-
-// One forward sweep over a table whose links are in range (check_tree): an
-// interior node's left child must come next, and after a leaf the innermost
-// pending right child; nothing may be left pending. The deepest leaf's
-// level is the depth.
-int check_preorder(pgpu_ctx* c, const pgpu_bvh_node* nodes, int n_nodes, int& depth) {
-    depth = 0;
-    if (n_nodes == 0) return PGPU_OK;
-    std::vector<int2>& pending = c->ws_size_height;   // (right child, its level)
-    pending.clear();
-    int level = 1;
-    for (int k = 0; k < n_nodes; ++k) {
+    int next_leaf = n_prims - 1, next_int = n_prims - 2;
+    for (int k = n_nodes - 1; k >= 0; --k) {
         const pgpu_bvh_node& nd = nodes[k];
-        if (nd.left >= 0) {
-            if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes)
-                return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
-            pending.push_back(make_int2(nd.right, level + 1));
-            ++level;
+        if (nd.left < 0) {
+            if (nd.right < 0 || nd.right >= n_prims)
+                return fail(c, PGPU_ERR_BVH_INVALID, "leaf %d references primitive %d", k, nd.right);
+            if (seen[nd.right]++)
+                return fail(c, PGPU_ERR_BVH_INVALID, "primitive %d is in two leaves", nd.right);
+            sh[k] = make_int2(1, 1);
+            idx[k] = next_leaf--;
             continue;
         }
-        depth = std::max(depth, level);
-        if (k + 1 == n_nodes) break;
-        if (pending.empty() || pending.back().x != k + 1)
-            return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k + 1);
-        level = pending.back().y;
-        pending.pop_back();
+        idx[k] = next_int--;
+        if (nd.left != k + 1 || nd.right <= nd.left || nd.right >= n_nodes ||
+            nd.right != nd.left + sh[nd.left].x)
+            return fail(c, PGPU_ERR_BVH_INVALID, "node %d is not in DFS pre-order", k);
+        sh[k] = make_int2(1 + sh[nd.left].x + sh[nd.right].x,
+                          1 + std::max(sh[nd.left].y, sh[nd.right].y));
     }
-    if (!pending.empty() || nodes[n_nodes - 1].left >= 0)
-        return fail(c, PGPU_ERR_BVH_INVALID, "unreachable nodes in table");
+    if (sh[0].x != n_nodes) return fail(c, PGPU_ERR_BVH_INVALID, "unreachable nodes in table");
+    depth = sh[0].y;
     if (depth > kMaxDepth)
         return fail(c, PGPU_ERR_UNSUPPORTED, "BVH depth %d exceeds %d", depth, kMaxDepth);
     return PGPU_OK;
@@ -767,7 +704,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         nodes = built.data();
         n_nodes = (int)built.size();
     }
-    int rc = check_tree(c, nodes, n_nodes, nU, depth, /*order=*/false);
+    int rc = check_tree(c, nodes, n_nodes, nU, depth);
     if (rc) return rc;
 
     // DFS order numbering of interior nodes and leaf slots (check_tree)
@@ -842,17 +779,8 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         const float* v = s->mesh_vertices + 3 * (size_t)i;
         return make_float4(v[0], v[1], v[2], 0.0f);
     };
-    // the table is read in order, but a node's right child and a leaf's
-    // primitive lie anywhere: they are fetched a few nodes ahead
-    constexpr int kAhead = 16;
     auto convert = [&](int kb, int ke) {
     for (int k = kb; k < ke; ++k) {
-        if (k + kAhead < ke) {
-            const pgpu_bvh_node& f = nodes[k + kAhead];
-            if (f.left >= 0) __builtin_prefetch(&nodes[f.right]);
-            else if (f.right < s->n_prims) __builtin_prefetch(&s->prims[f.right]);
-            else __builtin_prefetch(&s->mesh_indices[3 * (size_t)(f.right - s->n_prims)]);
-        }
         const pgpu_bvh_node& nd = nodes[k];
         if (nd.left >= 0) {
             const pgpu_bvh_node& L = nodes[nd.left];
@@ -905,21 +833,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         if (h_gc) h_gc[slot] = c;
     }
     };
-    // the sequential pre-order sweep runs beside the conversion, which reads
-    // nothing outside the table (its links are checked already)
-    {
-        const int C = std::max(1, std::min(4 * host_threads(), (n_nodes + 4095) / 4096));
-        const int chunk = (n_nodes + C - 1) / C;
-        host_run(C + 1, [&](int t) {
-            if (t == 0) {
-                rc = check_preorder(c, nodes, n_nodes, depth);
-                return;
-            }
-            const int b = (t - 1) * chunk, e = std::min(n_nodes, b + chunk);
-            if (b < e) convert(b, e);
-        });
-        if (rc) return rc;
-    }
+    parallel_for(n_nodes, convert);
 
     PGPU_CUDA(c, cudaSetDevice(c->device));
     auto ds = std::make_unique<DeviceScene>();
