@@ -710,8 +710,10 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     // DFS order numbering of interior nodes and leaf slots (check_tree)
     const std::vector<int>& idx = c->ws_idx;
     const int n_leaf = nU, n_int = nU > 0 ? nU - 1 : 0;
-    // triangles keep their three vertices in their leaf slot (geo_a, geo_b,
-    // geo_c): a triangle test then loads them directly, not via indices
+    // triangles keep their first vertex and both edges (v1 - v0, v2 - v0, the
+    // reference's first two operations, rounded alike here) in their leaf
+    // slot (geo_a, geo_b, geo_c): a triangle test then loads them directly,
+    // not via indices, and subtracts nothing
     const bool has_tri = s->n_mesh_triangles > 0 || first_bad(s->n_prims, [&](int k) {
         return s->prims[k].type == PGPU_PRIM_TRIANGLE;
     }) >= 0;
@@ -779,6 +781,10 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         const float* v = s->mesh_vertices + 3 * (size_t)i;
         return make_float4(v[0], v[1], v[2], 0.0f);
     };
+    // Triangle::hit's edge1 / edge2 (src/primitives.hpp:147-148): v - v0
+    auto edge = [](const float4& v0, const float4& v) {
+        return make_float4(v.x - v0.x, v.y - v0.y, v.z - v0.z, 0.0f);
+    };
     auto convert = [&](int kb, int ke) {
     for (int k = kb; k < ke; ++k) {
         const pgpu_bvh_node& nd = nodes[k];
@@ -801,8 +807,8 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
             const int t = prim - s->n_prims;
             h_lm[slot] = s->mesh_materials[t];
             a = vertex(s->mesh_indices[3 * t]);
-            b = vertex(s->mesh_indices[3 * t + 1]);
-            c = vertex(s->mesh_indices[3 * t + 2]);
+            b = edge(a, vertex(s->mesh_indices[3 * t + 1]));
+            c = edge(a, vertex(s->mesh_indices[3 * t + 2]));
         } else {
             const pgpu_prim& p = s->prims[prim];
             const float* q = p.p;
@@ -814,8 +820,8 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
                     break;
                 case PGPU_PRIM_TRIANGLE:
                     a = make_float4(q[0], q[1], q[2], 0.0f);
-                    b = make_float4(q[3], q[4], q[5], 0.0f);
-                    c = make_float4(q[6], q[7], q[8], 0.0f);
+                    b = edge(a, make_float4(q[3], q[4], q[5], 0.0f));
+                    c = edge(a, make_float4(q[6], q[7], q[8], 0.0f));
                     break;
                 case PGPU_PRIM_PLANE:
                     a = make_float4(q[0], q[1], q[2], 0.0f);

@@ -211,10 +211,11 @@ __device__ __forceinline__ bool hit_sphere(float4 g, const Ray& r, float tmin, f
 }
 
 // Triangle::hit, Moller-Trumbore (src/primitives.hpp:145-170)
+// The edges e1 = v1 - v0 and e2 = v2 - v0 come rounded as the reference
+// rounds them (the upload stores them in the leaf slot).
 template <bool REC>
-__device__ __forceinline__ bool hit_triangle(V3 v0, V3 v1, V3 v2, const Ray& r, float tmin,
+__device__ __forceinline__ bool hit_triangle(V3 v0, V3 e1, V3 e2, const Ray& r, float tmin,
                                              float tmax, float& t_out, Hit* h) {
-    V3 e1 = v1 - v0, e2 = v2 - v0;
     V3 hh = cross(r.d, e2);
     float a = dot(e1, hh);
     if (fabsf(a) < 1e-8f) return false;
