@@ -713,7 +713,8 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     // triangles keep their first vertex and both edges (v1 - v0, v2 - v0, the
     // reference's first two operations, rounded alike here) in their leaf
     // slot (geo_a, geo_b, geo_c): a triangle test then loads them directly,
-    // not via indices, and subtracts nothing
+    // not via indices, and subtracts nothing; the w words hold the face
+    // normal a hit record needs
     const bool has_tri = s->n_mesh_triangles > 0 || first_bad(s->n_prims, [&](int k) {
         return s->prims[k].type == PGPU_PRIM_TRIANGLE;
     }) >= 0;
@@ -785,6 +786,19 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     auto edge = [](const float4& v0, const float4& v) {
         return make_float4(v.x - v0.x, v.y - v0.y, v.z - v0.z, 0.0f);
     };
+    // the triangle's face normal, normalized(edge1 x edge2) with Vec3's
+    // operations in their order (src/vec3.hpp:56-68), in the w words of its
+    // three slot entries
+    auto put_normal = [](float4& a, float4& e1, float4& e2) {
+        const float nx = e1.y * e2.z - e1.z * e2.y;
+        const float ny = e1.z * e2.x - e1.x * e2.z;
+        const float nz = e1.x * e2.y - e1.y * e2.x;
+        const float len = std::sqrt(nx * nx + ny * ny + nz * nz);
+        const bool ok = len > 1e-12f;
+        a.w = ok ? nx / len : 0.0f;
+        e1.w = ok ? ny / len : 0.0f;
+        e2.w = ok ? nz / len : 0.0f;
+    };
     auto convert = [&](int kb, int ke) {
     for (int k = kb; k < ke; ++k) {
         const pgpu_bvh_node& nd = nodes[k];
@@ -809,6 +823,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
             a = vertex(s->mesh_indices[3 * t]);
             b = edge(a, vertex(s->mesh_indices[3 * t + 1]));
             c = edge(a, vertex(s->mesh_indices[3 * t + 2]));
+            put_normal(a, b, c);
         } else {
             const pgpu_prim& p = s->prims[prim];
             const float* q = p.p;
@@ -822,6 +837,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
                     a = make_float4(q[0], q[1], q[2], 0.0f);
                     b = edge(a, make_float4(q[3], q[4], q[5], 0.0f));
                     c = edge(a, make_float4(q[6], q[7], q[8], 0.0f));
+                    put_normal(a, b, c);
                     break;
                 case PGPU_PRIM_PLANE:
                     a = make_float4(q[0], q[1], q[2], 0.0f);

@@ -1137,8 +1137,8 @@ __device__ __forceinline__ bool any_hit4(const SceneView& S, const Ray& ray, flo
 
 // Full hit record of the closest hit found by closest_hit.
 // A sphere's or a triangle's record depends on the hit only through t: the
-// point is ray.at(t) and the normal follows from it (sphere) or from the
-// edges alone (triangle), as Sphere::hit / Triangle::hit make them
+// point is ray.at(t) and the normal follows from it (sphere) or is the
+// face's own (triangle), as Sphere::hit / Triangle::hit make them
 // (src/primitives.hpp:98-120, 145-170); the other primitives test again.
 __device__ __forceinline__ void make_hit(const SceneView& S, int best_ref, int slot,
                                          const Ray& ray, float tmin, float t_best, Hit& h) {
@@ -1151,10 +1151,12 @@ __device__ __forceinline__ void make_hit(const SceneView& S, int best_ref, int s
         h.p = ray.o + ray.d * t_best;
         set_face(h, ray, (h.p - v3(g.x, g.y, g.z)) / g.w);
     } else if (type == LEAF_TRIANGLE) {
-        const float4 b = __ldg(S.geo_b + s), c = __ldg(S.geo_c + s);
+        // the face normal, normalized(e1 x e2), stored by the upload in the
+        // w words of the slot
+        const float nx = __ldg(&S.geo_a[s].w), ny = __ldg(&S.geo_b[s].w), nz = __ldg(&S.geo_c[s].w);
         h.t = t_best;
         h.p = ray.o + ray.d * t_best;
-        set_face(h, ray, normalized(cross(v3(b.x, b.y, b.z), v3(c.x, c.y, c.z))));
+        set_face(h, ray, v3(nx, ny, nz));
     } else {
         float t;
         hit_leaf<true>(S, best_ref, ray, tmin, t_best, t, &h);
