@@ -372,9 +372,12 @@ __device__ __forceinline__ void warp_append(bool take, int slot, int* counter, i
     }
 }
 
-// ---- extend, camera rays of one scene: warp packets ------------------------------
+// ---- extend, camera rays: warp packets --------------------------------------------
 // The first bounce's queue holds the camera rays in slot order, so a warp's
-// 32 rays are the samples of two neighbouring pixels: nearly the same ray.
+// 32 rays are the samples of neighbouring pixels of one scene: nearly the same
+// ray (a batch's first queue is appended a generate warp at a time, so its
+// warps are mostly such groups too; a warp whose rays belong to different
+// scenes traces them one by one).
 // The warp traverses the wide tree once for all of them: every lane tests
 // every node the packet enters against its own ray and its own t_best, the
 // packet enters a child that any lane still reaches (nearest first by the
@@ -382,7 +385,7 @@ __device__ __forceinline__ void warp_append(bool take, int slot, int* counter, i
 // Node loads are broadcasts and all lanes stay busy. A lane still tests a
 // leaf only when its own slab test reaches it, so its result is the closest
 // hit among the same leaves as its own traversal would test.
-template <bool COUNT>
+template <bool COUNT, bool ONE>
 __global__ void __launch_bounds__(kWfMaxBlock) wf_extend_packet(WfArgs A) {
     __shared__ int s_ref[kWfMaxBlock / 32][kMaxStack];
     __shared__ float s_key[kWfMaxBlock / 32][kMaxStack];
@@ -392,13 +395,35 @@ __global__ void __launch_bounds__(kWfMaxBlock) wf_extend_packet(WfArgs A) {
     RayCount rc = {};
     const QView qv = qview(A, 0);
     unsigned int* cursor = A.work + 0;
-    const SceneView& S = A.view0;        // packets run in one-scene frames only
     while (true) {
         const int base = fetch32(cursor);
         if (base >= qv.total) break;
         const int e = base + lane;
         const bool valid = e < qv.total;
         const int slot = valid ? qv.slot(e) : -1;
+        int view = 0;
+        if constexpr (!ONE) {
+            view = valid ? A.jobs[A.st[slot].w].view : -1;
+            const int view0 = __shfl_sync(0xffffffffu, view, 0);   // lane 0 has a ray
+            if (!__all_sync(0xffffffffu, !valid || view == view0)) {
+                if (valid) {
+                    const SceneView& Sv = A.views[view];
+                    const float4 o = A.ray_o[slot], d = A.ray_d[slot];
+                    if (COUNT) rc.ext++;
+                    ClosestTrav4<0, COUNT> t1;
+                    TravStack<0> st1;
+                    if (!t1.init(Sv, Ray{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)}, 1e-4f, 1e9f,
+                                 &rc.tc))
+                        while (!t1.step(Sv, st1, &rc.tc)) {
+                        }
+                    A.hit[slot] = make_float4(t1.t_best, __int_as_float(t1.best_ref),
+                                              __int_as_float(t1.best), 0.0f);
+                }
+                continue;
+            }
+            view = view0;
+        }
+        const SceneView& S = ONE ? A.view0 : A.views[view];
         ClosestTrav4<kWfShared, COUNT> tr;
         bool active = false;
         if (valid) {
@@ -1036,7 +1061,7 @@ static cudaError_t occupancy(WfOccupancy& o, int blk = kWfBlock) {
     o.grid_accumulate = sms * 16 * kWfBlock / blk;
     int b4 = 0;
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, wf_extend_packet<COUNT>, blk, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, wf_extend_packet<COUNT, ONE>, blk, 0);
     o.grid_packet = sms * std::max(b4, 1);
     return e;
 }
@@ -1077,7 +1102,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
     WfOccupancy occ;
     cudaError_t e = occupancy<COUNT, ONE>(occ, blk);
     if (e != cudaSuccess) return e;
-    const bool packet_first = ONE && W.args.packets != 0;
+    const bool packet_first = W.args.packets != 0;
     // timed (profiled) frames stay on one stream so that kernel classes add
     // up; chunks of under 2^20 paths too, whose kernels are shorter than the
     // cross-stream waits would cost
@@ -1124,7 +1149,7 @@ static cudaError_t enqueue_frame(const WfScratch& W, const std::vector<WfJob>& j
         auto launch_extend = [&](int it) {
             lt.mark(KC_EXTEND, st, true);
             if (it == 0 && packet_first)
-                wf_extend_packet<COUNT><<<occ.grid_packet, blk, 0, st>>>(A);
+                wf_extend_packet<COUNT, ONE><<<occ.grid_packet, blk, 0, st>>>(A);
             else
                 wf_extend<COUNT, ONE><<<occ.grid_extend, blk, smem, st>>>(A, it);
             lt.mark(KC_EXTEND, st, false);
