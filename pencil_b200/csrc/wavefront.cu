@@ -265,8 +265,9 @@ wf_generate(WfArgs A, long long path_begin, int n_slots) {
         Ray r = camera_ray(S.cam, u, v);
         A.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
         A.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
-        A.T[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-        A.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        // a path's first shade (iteration 0) starts from T = 1, L = 0 without
+        // loading them; only a path that is never shaded needs its L here
+        if (P.depth <= 0) A.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         A.rec[(size_t)slot * 4 + 3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));  // nothing pending
         uint32_t flags = P.mode == kModeWhitted ? kFlagWhitted : 0u;
         A.st[slot] = make_uint4(rng.s, (unsigned)P.depth, flags, (unsigned)jb);
@@ -580,7 +581,9 @@ wf_shade(WfArgs A, int it) {
             uint4 stv = A.st[slot];
             const WfJob& J = job_of<ONE>(A, stv.w);
             const SceneView& S = view_of<ONE>(A, stv.w);
-            float4 o = A.ray_o[slot], d = A.ray_d[slot], T = A.T[slot], L = A.L[slot];
+            const float4 o = A.ray_o[slot], d = A.ray_d[slot];
+            const float4 T = it == 0 ? make_float4(1.0f, 1.0f, 1.0f, 0.0f) : A.T[slot];
+            const float4 L = it == 0 ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : A.L[slot];
             float4 hv = A.hit[slot];
             PathState ps;
             ps.ray = Ray{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z)};
