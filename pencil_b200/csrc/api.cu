@@ -685,6 +685,10 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
                 return fail(c, PGPU_ERR_INVALID_ARG, "quad light %d material out of range", k);
             HV cr = hcross(hv(l.edge_u), hv(l.edge_v));
             d.area = std::sqrt(cr.x * cr.x + cr.y * cr.y + cr.z * cr.z);
+            const HV nq = hnorm(cr);     // the device's normalized(), same operations
+            d.normal[0] = nq.x;
+            d.normal[1] = nq.y;
+            d.normal[2] = nq.z;
             if (!(d.area > 0.0f)) return fail(c, PGPU_ERR_INVALID_ARG, "quad light %d has no area", k);
             quad_mats.push_back(l.material);
             has_quad = 1;

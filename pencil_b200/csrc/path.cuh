@@ -156,7 +156,7 @@ __device__ __forceinline__ bool quad_sample(const DevLight& l, V3 p, V3 n, V3 so
     L = d / dist;
     float cx = dot(n, L);
     if (cx <= 0.0f) return false;
-    V3 nq = normalized(cross(ld3(l.edge_u), ld3(l.edge_v)));
+    const V3 nq = ld3(l.normal);      // normalized(edge_u x edge_v), from the upload
     float ly = dot(nq, L);
     float cy = fabsf(ly);
     w = cx * cy * l.area / (3.14159265f * d2);

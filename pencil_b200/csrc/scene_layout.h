@@ -101,6 +101,7 @@ struct alignas(16) DevLight {
     float edge_u[3];
     float edge_v[3];
     float area;            // quad: |edge_u x edge_v|
+    float normal[3];       // quad: normalized(edge_u x edge_v)
 };
 
 // Everything a kernel needs to trace one scene; passed by value for
