@@ -717,8 +717,8 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     // triangles keep their first vertex and both edges (v1 - v0, v2 - v0, the
     // reference's first two operations, rounded alike here) in their leaf
     // slot (geo_a, geo_b, geo_c): a triangle test then loads them directly,
-    // not via indices, and subtracts nothing; geo_n holds the face normal
-    // and material a hit record needs
+    // not via indices, and subtracts nothing; the w words hold the face
+    // normal a hit record needs
     const bool has_tri = s->n_mesh_triangles > 0 || first_bad(s->n_prims, [&](int k) {
         return s->prims[k].type == PGPU_PRIM_TRIANGLE;
     }) >= 0;
@@ -738,8 +738,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     size_t off_gb = align256(off_ga + (size_t)n_leaf * 16);
     size_t off_gc = align256(off_gb + (size_t)n_leaf * 16);
     const size_t gc_bytes = has_tri ? (size_t)n_leaf * 16 : 0;
-    size_t off_gn = align256(off_gc + gc_bytes);
-    size_t off_lm = align256(off_gn + gc_bytes);
+    size_t off_lm = align256(off_gc + gc_bytes);
     size_t off_lp = align256(off_lm + (size_t)n_leaf * 4);
     size_t off_mt = align256(off_lp + (size_t)n_leaf * 4);
     size_t off_lt = align256(off_mt + (size_t)s->n_materials * sizeof(DevMaterial));
@@ -762,8 +761,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         const size_t ends[][2] = {{off_nodes + (size_t)n_int * 64, off_ga},
                                   {off_ga + (size_t)n_leaf * 16, off_gb},
                                   {off_gb + (size_t)n_leaf * 16, off_gc},
-                                  {off_gc + gc_bytes, off_gn},
-                                  {off_gn + gc_bytes, off_lm},
+                                  {off_gc + gc_bytes, off_lm},
                                   {off_lm + (size_t)n_leaf * 4, off_lp},
                                   {off_lp + (size_t)n_leaf * 4, off_mt},
                                   {off_mt + (size_t)s->n_materials * sizeof(DevMaterial), off_lt},
@@ -775,7 +773,6 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     float4* h_ga = reinterpret_cast<float4*>(host + off_ga);
     float4* h_gb = reinterpret_cast<float4*>(host + off_gb);
     float4* h_gc = has_tri ? reinterpret_cast<float4*>(host + off_gc) : nullptr;
-    float4* h_gn = has_tri ? reinterpret_cast<float4*>(host + off_gn) : nullptr;
     int* h_lm = reinterpret_cast<int*>(host + off_lm);
     int* h_lp = reinterpret_cast<int*>(host + off_lp);
     DevMaterial* h_mt = reinterpret_cast<DevMaterial*>(host + off_mt);
@@ -793,19 +790,18 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     auto edge = [](const float4& v0, const float4& v) {
         return make_float4(v.x - v0.x, v.y - v0.y, v.z - v0.z, 0.0f);
     };
-    // a triangle's hit-record words: its face normal, normalized(edge1 x
-    // edge2) with Vec3's operations in their order (src/vec3.hpp:56-68), and
-    // its material, in one 16-byte entry (one sector per shaded vertex)
-    auto face = [](const float4& e1, const float4& e2, int mat) {
+    // the triangle's face normal, normalized(edge1 x edge2) with Vec3's
+    // operations in their order (src/vec3.hpp:56-68), in the w words of its
+    // three slot entries
+    auto put_normal = [](float4& a, float4& e1, float4& e2) {
         const float nx = e1.y * e2.z - e1.z * e2.y;
         const float ny = e1.z * e2.x - e1.x * e2.z;
         const float nz = e1.x * e2.y - e1.y * e2.x;
         const float len = std::sqrt(nx * nx + ny * ny + nz * nz);
         const bool ok = len > 1e-12f;
-        int m = mat;
-        float mw;
-        std::memcpy(&mw, &m, 4);
-        return make_float4(ok ? nx / len : 0.0f, ok ? ny / len : 0.0f, ok ? nz / len : 0.0f, mw);
+        a.w = ok ? nx / len : 0.0f;
+        e1.w = ok ? ny / len : 0.0f;
+        e2.w = ok ? nz / len : 0.0f;
     };
     auto convert = [&](int kb, int ke) {
     for (int k = kb; k < ke; ++k) {
@@ -824,7 +820,6 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
         const int slot = idx[k];
         const int prim = nd.right;
         h_lp[slot] = prim;
-        if (h_gn) h_gn[slot] = zero;           // triangles fill theirs below
         float4 a = zero, b = zero, c = zero;
         if (prim >= s->n_prims) {
             const int t = prim - s->n_prims;
@@ -832,7 +827,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
             a = vertex(s->mesh_indices[3 * t]);
             b = edge(a, vertex(s->mesh_indices[3 * t + 1]));
             c = edge(a, vertex(s->mesh_indices[3 * t + 2]));
-            h_gn[slot] = face(b, c, s->mesh_materials[t]);
+            put_normal(a, b, c);
         } else {
             const pgpu_prim& p = s->prims[prim];
             const float* q = p.p;
@@ -846,7 +841,7 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
                     a = make_float4(q[0], q[1], q[2], 0.0f);
                     b = edge(a, make_float4(q[3], q[4], q[5], 0.0f));
                     c = edge(a, make_float4(q[6], q[7], q[8], 0.0f));
-                    h_gn[slot] = face(b, c, p.material);
+                    put_normal(a, b, c);
                     break;
                 case PGPU_PRIM_PLANE:
                     a = make_float4(q[0], q[1], q[2], 0.0f);
@@ -947,7 +942,6 @@ int32_t pgpu_upload_scene(pgpu_ctx* c, const pgpu_scene* s, int32_t* out_id) {
     v.geo_a = reinterpret_cast<const float4*>(base + off_ga);
     v.geo_b = reinterpret_cast<const float4*>(base + off_gb);
     v.geo_c = has_tri ? reinterpret_cast<const float4*>(base + off_gc) : nullptr;
-    v.geo_n = has_tri ? reinterpret_cast<const float4*>(base + off_gn) : nullptr;
     v.leaf_mat = reinterpret_cast<const int*>(base + off_lm);
     v.leaf_prim = reinterpret_cast<const int*>(base + off_lp);
     v.mats = reinterpret_cast<const DevMaterial*>(base + off_mt);

@@ -1151,14 +1151,12 @@ __device__ __forceinline__ void make_hit(const SceneView& S, int best_ref, int s
         h.p = ray.o + ray.d * t_best;
         set_face(h, ray, (h.p - v3(g.x, g.y, g.z)) / g.w);
     } else if (type == LEAF_TRIANGLE) {
-        // the face normal, normalized(e1 x e2), and the material, stored by
-        // the upload side by side
-        const float4 nm = __ldg(S.geo_n + s);
+        // the face normal, normalized(e1 x e2), stored by the upload in the
+        // w words of the slot
+        const float nx = __ldg(&S.geo_a[s].w), ny = __ldg(&S.geo_b[s].w), nz = __ldg(&S.geo_c[s].w);
         h.t = t_best;
         h.p = ray.o + ray.d * t_best;
-        set_face(h, ray, v3(nm.x, nm.y, nm.z));
-        h.mat = __float_as_int(nm.w);
-        return;
+        set_face(h, ray, v3(nx, ny, nz));
     } else {
         float t;
         hit_leaf<true>(S, best_ref, ray, tmin, t_best, t, &h);

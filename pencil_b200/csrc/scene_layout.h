@@ -25,23 +25,20 @@
 //             [7G .. 8G)      = unused
 //   geo_a   float4[n_leaves]        leaf geometry in DFS leaf order (slot):
 //             sphere   (center.xyz, radius)
-//             triangle (v0.xyz, -)
+//             triangle (v0.xyz, face normal x)
 //             cube     (center.xyz, half)
 //             plane    (point.xyz, -)
 //             cylinder (center.xyz, radius)
 //             cone     (apex.xyz, radius)
 //   geo_b   float4[n_leaves]        second word where needed (zero elsewhere):
-//             triangle (v1 - v0, -)
+//             triangle (v1 - v0, face normal y)
 //             plane    (normal.xyz, -)
 //             cylinder (axis.xyz, half_height)
 //             cone     (axis.xyz, height)
 //   geo_c   float4[n_leaves]        only in scenes with triangles:
-//             triangle (v2 - v0, -)
+//             triangle (v2 - v0, face normal z)
 //           (a triangle's first vertex and edges sit in its slot, so its
 //            test loads them at once instead of through an index word)
-//   geo_n   float4[n_leaves]        only in scenes with triangles: a
-//             triangle's face normal normalized(e1 x e2) and its material
-//             (int bits in w), the words its hit record needs, in one sector
 //   leaf_mat  int32[n_leaves]       material id per slot
 //   leaf_prim int32[n_leaves]       caller's primitive index per slot
 //   mats    DevMaterial[n_materials]
@@ -115,8 +112,6 @@ struct SceneView {
     const float4* geo_a;
     const float4* geo_b;
     const float4* geo_c;   // null in scenes without triangles
-    const float4* geo_n;   // triangles: face normal xyz, material (int bits); null
-                           // in scenes without triangles
     const int* leaf_mat;
     const int* leaf_prim;
     const DevMaterial* mats;
