@@ -156,6 +156,9 @@ def test_invalid_launch_shapes_are_rejected(gpu):
         expect(A.ERR_INVALID_ARG, gpu.render, sid, dataclasses.replace(ST, block_size=bs),
                match="block_size")
     expect(A.ERR_INVALID_ARG, gpu.render, sid, dataclasses.replace(ST, refill_below=40))
+    for q in (-1, (1 << 28) + 1):
+        expect(A.ERR_INVALID_ARG, gpu.render, sid, dataclasses.replace(ST, queue_capacity=q),
+               match="queue_capacity")
     for bs in (64, 128, 256):          # every supported shape gives the same image
         a = gpu.render(sid, dataclasses.replace(ST, block_size=bs, sort_key=3))
         assert np.array_equal(a.view(np.uint32), gpu.render(sid, ST).view(np.uint32))
