@@ -69,8 +69,9 @@ def parse_args():
                     help="skip the adjoint, batch and image-quality measurements")
     ap.add_argument("--profile-pencil-tree", action="store_true",
                     help="mesh profile case: the wide traversals on Pencil's tree")
-    ap.add_argument("--profile-case", choices=["wavefront", "megakernel", "mesh", "adjoint",
-                                               "lbvh", "tonemap"], default=None,
+    ap.add_argument("--profile-case", choices=["wavefront", "megakernel", "mesh",
+                                               "mesh_megakernel", "adjoint", "lbvh", "tonemap"],
+                    default=None,
                     help="render the workload once, kernels launched one by one (for ncu)")
     ap.add_argument("--profile-scale", type=int, default=1,
                     help="divide the image width and height by this (smaller ncu cases)")
@@ -875,7 +876,7 @@ def run_profile_case(args) -> None:
         print(json.dumps(out))
         ctx.close()
         return
-    mesh = args.profile_case == "mesh"
+    mesh = args.profile_case in ("mesh", "mesh_megakernel")
     wl = W.mesh_box() if mesh else W.sphere_cloud()
     st = wl.settings
     st.width //= args.profile_scale
@@ -889,7 +890,8 @@ def run_profile_case(args) -> None:
     st.queue_capacity = st.width * st.height * st.samples ** 2
     st.refill_below = 20 if mesh else 16
     st.sort_key = 3
-    st.engine = A.ENGINE_MEGAKERNEL if args.profile_case == "megakernel" else A.ENGINE_WAVEFRONT
+    st.engine = (A.ENGINE_MEGAKERNEL if args.profile_case in ("megakernel", "mesh_megakernel")
+                 else A.ENGINE_WAVEFRONT)
     ctx = GpuContext(0)
     if mesh and not args.profile_pencil_tree:
         ctx.set_traversal_tree(A.TRAVERSAL_LBVH)
