@@ -379,6 +379,13 @@ def run_ours(args) -> None:
         roof["l2_frac"] = ncu["l2_throughput_pct"] / 100.0
     if "l1_lsu_wavefronts_pct" in ncu:
         roof["l1_data_pipe_frac"] = ncu["l1_lsu_wavefronts_pct"] / 100.0
+    # the memory level the counters show busiest: "bound" keeps the class
+    # (memory, no tensor work); this names the unit and its busy fraction
+    levels = {k: roof[f] for k, f in (("dram", "dram_frac"), ("l2", "l2_frac"),
+                                      ("l1_data_pipe", "l1_data_pipe_frac")) if f in roof}
+    if levels:
+        top = max(levels, key=levels.get)
+        roof["bound_by_counters"] = {"unit": top, "frac": levels[top]}
     roof["limiter"] = ("the L1 data pipe serving scattered node loads (its lsu wavefronts at "
                        "l1_data_pipe_frac of peak in one ncu launch) and the latency of those "
                        "loads (long-scoreboard stalls); DRAM and L2 fractions well below 1, and "
@@ -665,7 +672,8 @@ def measure_quality(ctx, sid, st, stream) -> dict:
     image is the reference's own estimator -- trace_path with both
     dielectric branches (the megakernel's exact glass mode) -- at 4096 spp,
     as 64 renders of 64 spp with distinct sample offsets. Mesh box (the
-    displaced icosphere, quad light) at 256x256: reference 32768 spp of the
+    displaced icosphere, quad light) at 256x256, the wavefront with the
+    launch parameters the autotuner picks for that frame: reference 32768 spp of the
     production estimator (32 renders of 1024 spp; at 4096 spp its own noise,
     1.3%, would hide the 1% criterion), the point searched up to 16384 spp; the reference's own estimator (BSDF sampling only: the small emitter
     is found by chance) at 4096 spp is measured against it too."""
@@ -689,12 +697,21 @@ def measure_quality(ctx, sid, st, stream) -> dict:
     finally:
         ctx.set_traversal_tree(A.TRAVERSAL_UPLOADED)
     sm_st = dataclasses.replace(wm.settings, engine=A.ENGINE_WAVEFRONT)
+    # the wavefront's launch parameters for this frame shape (1024 spp, one
+    # render of the search), as the renderer would pick them
+    from pencil_b200.autotune import autotune
+    tune_st = dataclasses.replace(sm_st, samples=32)
+    tuned = autotune(ctx, [sm], [tune_st], scene=wm.scene, reps=1, use_cache=False)
+    for k in ("queue_capacity", "refill_below", "sort_key", "block_size"):
+        setattr(sm_st, k, tuned[k])
     mwin = (0, 0, 256, 256)
     t0 = time.perf_counter()
     mref, mnoise, _ = _reference_image(ctx, sm, sm_st, mwin, frames=32, n=32)
     rec = {"workload": "mesh_box at 256x256, depth 12",
            "reference": "production estimator (quad-light NEE), 32768 spp",
            "reference_seconds": time.perf_counter() - t0,
+           "autotuned": {k: tuned[k] for k in ("queue_capacity", "refill_below", "sort_key",
+                                                "block_size", "ms")},
            **_equal_rmse_point(ctx, sm, sm_st, mwin, mref, mnoise, max_spp=16384,
                               ref_spp=32768)}
     # the reference's own estimator (no quad light: BSDF sampling only) at
@@ -789,6 +806,12 @@ def measure_mesh(ctx, stream) -> dict:
         st.count_rays, st.count_nodes = True, True
         ctx.render(sid, st, stats=cnt)
         st.count_rays, st.count_nodes = False, False
+        # device time per kernel class (kernels launched one by one, events
+        # around each; outside the timed frames)
+        prof = RenderStats()
+        st.profile_kernels = True
+        ctx.render(sid, st, stats=prof)
+        st.profile_kernels = False
         st.engine = A.ENGINE_MEGAKERNEL
         mk = _event_ms(stream, lambda: ctx.render_device(sid, st, buf.data_ptr()), 1)
         st.engine = A.ENGINE_WAVEFRONT
@@ -797,8 +820,12 @@ def measure_mesh(ctx, stream) -> dict:
                 "wavefront_mrays_s": rays / wf / 1e3,
                 "megakernel_ms": mk, "megakernel_mpaths_s": paths / mk / 1e3,
                 "wavefront_over_megakernel": mk / wf,
+                "kernel_ms": {k: round(v, 3) for k, v in prof.kernel_ms.items() if v > 0},
                 "ext_node_visits_per_ray": cnt.ext_node_visits / max(1, cnt.extension_rays),
-                "shadow_node_visits_per_ray": cnt.shadow_node_visits / max(1, cnt.shadow_rays)}
+                "shadow_node_visits_per_ray": cnt.shadow_node_visits / max(1, cnt.shadow_rays),
+                # leaf records read by leaf tests (48 B per triangle)
+                "ext_leaf_bytes_per_ray": cnt.ext_leaf_bytes / max(1, cnt.extension_rays),
+                "shadow_leaf_bytes_per_ray": cnt.shadow_leaf_bytes / max(1, cnt.shadow_rays)}
 
     # the renderer's configuration: LBVH traversal tree over Pencil's leaves
     ctx.set_traversal_tree(A.TRAVERSAL_LBVH)
