@@ -5,11 +5,12 @@
 // counter-RNG seeds: the same camera rays, hits, next-event samples, Russian
 // roulette decisions and scatter directions as the production renderer
 // (shade_vertex in path.cuh; the control flow and random-number use below
-// follow it step for step), traced on Pencil's binary tree (in its
-// child-pair layout: at 128 registers the replay ran 21 ms per gradient there
-// against 27 ms on the 4-wide tree). No state of the forward render is kept: the
-// replay records a short tape per path (at most kMaxTape vertices) and sweeps
-// it backwards.
+// follow it step for step), traced on the 4-wide tree the renderers walk
+// (the same hits as Pencil's binary tree; at 80 registers, six blocks per
+// SM, 17.5 ms per gradient there against 19.8 ms on the binary tree -- at
+// 128 registers the binary tree had been the faster). No state of the
+// forward render is kept: the replay records a short tape per path (at most
+// kMaxTape vertices) and sweeps it backwards.
 //
 // Per colour channel a path's radiance is L = sum_k T_k * A_k with
 // T_{k+1} = T_k * f_k. At vertex k with material m and albedo a:
@@ -94,7 +95,7 @@ struct Replay {
 
     __device__ __forceinline__ bool occluded(const Ray& r, float tmin, float tmax) {
         if (COUNT) rc.shadow++;
-        return any_hit<kAdjShared, COUNT>(S, r, tmin, tmax, stk, &rc.tc);
+        return any_hit4<kAdjShared, COUNT>(S, r, tmin, tmax, stk, &rc.tc);
     }
 
     // Replay one path; fills the tape (returns its length; each vertex with
@@ -116,7 +117,7 @@ struct Replay {
             if (COUNT) rc.ext++;
             float tb;
             int bref;
-            int slot = closest_hit<kAdjShared, COUNT>(S, r, 1e-4f, 1e9f, tb, bref, stk, &rc.tc);
+            int slot = closest_hit4<kAdjShared, COUNT>(S, r, 1e-4f, 1e9f, tb, bref, stk, &rc.tc);
             if (slot < 0) {
                 tv.mat = -1;
                 tv.A = ld3(S.bg);
