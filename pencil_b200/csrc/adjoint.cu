@@ -271,10 +271,10 @@ struct Replay {
     }
 };
 
-// Held to 80 registers (six blocks of 128 threads per SM): the tape lives in
-// local memory either way, and the extra resident warps hide more of its
-// latency (19.9 against 20.3 ms per gradient at 128 registers).
-constexpr int kAdjMinBlocks = 6;
+// Held to 72 registers (seven blocks of 128 threads per SM): the tape lives
+// in local memory either way, and the extra resident warps hide more of its
+// latency (per gradient: 16.45 ms; 17.49 at 80 registers, 16.70 at 64).
+constexpr int kAdjMinBlocks = 7;
 
 template <bool COUNT>
 __global__ void __launch_bounds__(kAdjBlock, kAdjMinBlocks)
