@@ -17,9 +17,15 @@
 namespace pgpu {
 
 constexpr int kMkShared = 16;   // stack entries per thread kept in shared memory
+// Held to 64 registers (eight blocks of 128 threads per SM): more resident
+// warps hide more of the divergent paths' load latency than the spilled
+// words cost. Sphere-cloud frame 85.8 ms at the compiler's choice (96-128
+// registers) -> 73.4 at 72 -> 71.8 at 64; mesh frame 443.5 -> 378.0 ->
+// 382.3 ms.
+constexpr int kMkMinBlocks = 8;
 
 template <bool COUNT, bool TREE, bool PIXEL_SEQ, bool WIDE>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, kMkMinBlocks)
 mk_render(SceneView S, PathParams P, int G, float* __restrict__ out, float* __restrict__ m2,
           unsigned long long* __restrict__ counters) {
     extern __shared__ int smem[];
