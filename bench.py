@@ -75,6 +75,9 @@ def parse_args():
                     help="render the workload once, kernels launched one by one (for ncu)")
     ap.add_argument("--profile-scale", type=int, default=1,
                     help="divide the image width and height by this (smaller ncu cases)")
+    ap.add_argument("--arena-sizes", action="store_true",
+                    help="traversal cost per node visit on mesh arenas of 15 MB to 1 GB "
+                         "(one JSON line per size)")
     ap.add_argument("--profile-counts", action="store_true",
                     help="with --profile-case: also render once with ray counters and "
                          "print them (run without ncu)")
@@ -874,6 +877,55 @@ class _Null:
         return False
 
 
+def run_arena_sizes() -> None:
+    """Traversal cost per node visit against scene-arena size: the mesh box
+    with icospheres of 6..9 subdivisions (81,920 to 5,242,880 triangles),
+    512x512, 64 spp, depth 12, on Pencil's tree collapsed to 4-wide nodes;
+    the wavefront with one chunk of 2^24 paths, refill 16, sort key 3,
+    64-thread blocks. Per size: the frame on both engines (CUDA events), the
+    kernel-class times (events around each class, a second render) and the
+    node visits (the counting build), one JSON line each."""
+    import torch
+    from pencil_b200 import _abi as A
+    from pencil_b200 import workloads as W
+    from pencil_b200.renderer import GpuContext, RenderStats
+    ctx = GpuContext(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    for subdiv in (6, 7, 8, 9):
+        wm = W.mesh_box(subdiv=subdiv, width=512, height=512, samples=8, depth=12)
+        nodes, _ = wm.scene.build_bvh()
+        sid = ctx.upload(wm.scene, nodes)
+        info = ctx.scene_info(sid)
+        st = wm.settings
+        st.engine = A.ENGINE_WAVEFRONT
+        st.queue_capacity, st.refill_below, st.sort_key, st.block_size = 1 << 24, 16, 3, 64
+        buf = torch.empty((st.height, st.width, 3), dtype=torch.float32, device="cuda")
+        wf = _event_ms(stream, lambda: ctx.render_device(sid, st, buf.data_ptr()), 2)
+        prof = RenderStats()
+        st.profile_kernels = True
+        ctx.render(sid, st, stats=prof)
+        ctx.render(sid, st, stats=prof)
+        st.profile_kernels = False
+        cnt = RenderStats()
+        st.count_rays, st.count_nodes = True, True
+        ctx.render(sid, st, stats=cnt)
+        st.count_rays, st.count_nodes = False, False
+        st.engine = A.ENGINE_MEGAKERNEL
+        mk = _event_ms(stream, lambda: ctx.render_device(sid, st, buf.data_ptr()), 1)
+        km = prof.kernel_ms
+        print(json.dumps({
+            "subdiv": subdiv, "triangles": int(len(wm.scene.mesh_indices)),
+            "arena_mb": info["device_bytes"] / 2 ** 20, "wide_nodes": info["n_wide"],
+            "ext_visits_per_ray": cnt.ext_node_visits / max(1, cnt.extension_rays),
+            "shadow_visits_per_ray": cnt.shadow_node_visits / max(1, cnt.shadow_rays),
+            "extend_ms": km["extend"], "shadow_ms": km["shadow"],
+            "ps_per_ext_visit": km["extend"] * 1e9 / max(1, cnt.ext_node_visits),
+            "ps_per_shadow_visit": km["shadow"] * 1e9 / max(1, cnt.shadow_node_visits),
+            "wavefront_ms": wf, "megakernel_ms": mk, "ratio": mk / wf}), flush=True)
+        ctx.free(sid)
+    ctx.close()
+
+
 def run_profile_case(args) -> None:
     """One frame of the workload with no CUDA graph, for ncu captures (or one
     adjoint of the box configuration, one device BVH build of the sphere
@@ -943,6 +995,8 @@ def main():
     args = parse_args()
     if args.profile_case:
         run_profile_case(args)
+    elif args.arena_sizes:
+        run_arena_sizes()
     elif args.impl == "reference":
         run_reference(args)
     else:
