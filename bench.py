@@ -163,6 +163,27 @@ def cpu_reference_run(scene, steps: int, warmup: int) -> dict:
             "seconds": secs}
 
 
+def cpu_batch_sample(jobs) -> dict:
+    """The reference CPU renderer on a seeded subset of the batch's scenes
+    (one run each, all host threads), as a per-path rate."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    if not O.ref_available():
+        return {"value": None, "unit": "Mpaths/s", "cores": threads, "kind": "reference",
+                "sample": "unavailable: the reference renderer is not built"}
+    secs, paths = 0.0, 0
+    for j in jobs:
+        st = j.settings
+        _, info = O.ref_render(j.scene, st.width, st.height, st.samples, st.pathtrace_bounces,
+                               True, threads=threads, repeat=1, want_image=False)
+        secs += float(info["seconds"][0])
+        paths += st.width * st.height * st.samples ** 2
+    return {"value": paths / secs / 1e6, "unit": "Mpaths/s", "cores": threads,
+            "kind": "reference", "scenes": len(jobs), "paths": paths, "seconds": secs,
+            "sample": f"every 32nd of the 256 scenes ({len(jobs)}), one run each, "
+                      "extrapolated per path"}
+
+
 def reference_order_counts(scene, settings) -> dict:
     """Algorithmic work per ray of the frame's paths, counted by the oracle
     on COUNT_WINDOW: its replay of the production estimator walks Pencil's
@@ -582,6 +603,10 @@ def measure_extras(ctx, sid, st, img, stream) -> dict:
                     "one_by_one_megakernel_ms": mk_ms}
     for s_ in sids:
         ctx.free(s_)
+    try:
+        out["batch"]["cpu_baseline"] = cpu_batch_sample(jobs[::32])
+    except Exception as ex:  # noqa: BLE001
+        out["batch"]["cpu_baseline"] = {"value": None, "sample": f"failed: {ex}"}
     out["mesh"] = measure_mesh(ctx, stream)
     out["bvh_build"] = measure_bvh_build(ctx, stream)
     return out
